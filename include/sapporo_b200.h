@@ -1,0 +1,140 @@
+/*
+ * sapporo_b200.h -- the thin C ABI between the host library (the sapporo
+ * class and the GRAPE-6 g6_* interface) and the B200 device code.
+ *
+ * Plain C types only; every function returns 0 on success or a negative
+ * SAPB_E* code (see sapb_error_string).  One sapb_dev owns one GPU's state
+ * and one CUDA stream.  Not thread-safe per handle.
+ *
+ * Each entry point names the reference interface whose role it takes
+ * (reference file:line, paths relative to the reference tree).
+ */
+#ifndef SAPPORO_B200_H
+#define SAPPORO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SAPB_OK 0
+#define SAPB_ECUDA (-1)     /* a CUDA runtime call failed */
+#define SAPB_EINVAL (-2)    /* invalid argument or state */
+#define SAPB_ENOMEM (-3)    /* device or pinned allocation failed */
+#define SAPB_ETIMEOUT (-4)  /* a device-side bounded wait gave up */
+#define SAPB_ENODEV (-5)    /* no usable CUDA device */
+
+/* integration order / precision, same values as lib/include/defines.h:30-31 */
+#define SAPB_GRAPE5 0
+#define SAPB_FOURTH 1
+#define SAPB_SIXTH 2
+#define SAPB_FLOAT 0
+#define SAPB_DOUBLESINGLE 1
+#define SAPB_DOUBLE 2
+
+#define SAPB_NGB_PB 256      /* neighbour slots per i, lib/include/defines.h:9 */
+#define SAPB_NPIPES 16384    /* default i per call, lib/include/defines.h:14 */
+#define SAPB_RES_STRIDE 12   /* doubles per result record */
+
+/* result record (SAPB_RES_STRIDE doubles per i):
+ *   [0..2] acc  [3] pot  [4..6] jerk  [7..9] snap  [10] ds2 of the nearest
+ *   neighbour (float precision, 1e11 if none)  [11] its id (-1 if none)   */
+
+/* flags for sapb_force */
+#define SAPB_F_PREDICT 1    /* run the predictor to t_i first */
+#define SAPB_F_NGB_LIST 2   /* build neighbour lists */
+
+typedef struct sapb_dev sapb_dev;
+
+/* Library build / error helpers. */
+const char *sapb_version(void);
+const char *sapb_error_string(int code);
+const char *sapb_last_error(const sapb_dev *d); /* detail of the last failure */
+int sapb_device_count(int *count);
+
+/* Opens `device` for the given order/precision.  Replaces
+ * sapporo::open (lib/src/sapporohostclass.cpp:90-372) together with
+ * device::assignDevice / allocateMemory (lib/include/sapdevclass.h:122-273).
+ * n_pipes: maximum i per force call (<= 0: SAPB_NPIPES);
+ * nj_reserve: initial j capacity (<= 0: 16384, as the reference). */
+int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
+              int nj_reserve);
+int sapb_close(sapb_dev *d);
+int sapb_info(const sapb_dev *d, int *order, int *precision, int *n_pipes, int *j_capacity,
+              int *num_sms);
+
+/* Uses an external cudaStream_t (passed as void*) for all work; NULL
+ * restores the library's own stream. */
+int sapb_set_stream(sapb_dev *d, void *stream);
+
+/* Grows the device j capacity, keeping the stored j.  Replaces
+ * sapporo::increase_jMemory / device::reallocJParticles
+ * (lib/src/sapporohostclass.cpp:560-583, lib/include/sapdevclass.h:275-325). */
+int sapb_reserve_j(sapb_dev *d, int nj_capacity);
+
+/* Pinned host staging for updated j-particles: returns a pointer to room for
+ * `n` records of sapb_j_stage_stride() doubles (contents preserved on
+ * growth), or NULL.  Record layout:
+ *   [0] address (low 32 bits) | id (high 32 bits)  [1] t  [2] mass
+ *   [3..5] x  [6..8] v  [9..11] acc  [12..14] jerk  [15] eps
+ *   [16..18] snap  [19..21] crackle   (6th order only)
+ * Plays the role of the *_temp host mirrors written by
+ * sapporo::set_j_particle (lib/src/sapporohostclass.cpp:500-516). */
+double *sapb_j_stage(sapb_dev *d, int n);
+int sapb_j_stage_stride(const sapb_dev *d);
+
+/* Copies the first n staged records to the device and scatters them to their
+ * addresses (asynchronous).  Replaces send_j_particles_to_device + copyJInDev
+ * (lib/src/sapporohostclass.cpp:889-923, 1204-1248). */
+int sapb_push_j(sapb_dev *d, int n);
+
+/* Predicts j[0, nj) to t_i (asynchronous).  Replaces predictJParticles
+ * (lib/src/sapporohostclass.cpp:1250-1284). */
+int sapb_predict(sapb_dev *d, int nj, double ti);
+
+/* Pinned host buffer for `ni` i records (8 doubles each for 4th order:
+ * x0 x1 x2 h2 v0 v1 v2 id-bits; 12 for 6th: + a0 a1 a2 0).  The id is
+ * stored in the low 32 bits of slot 7. */
+double *sapb_i_stage(sapb_dev *d, int ni);
+int sapb_i_stage_stride(const sapb_dev *d);
+
+/* Force on the ni staged i-particles from j[0, nj): H2D of the i records,
+ * optional prediction to ti, force kernels, D2H of the results into pinned
+ * memory -- all asynchronous on the device stream.  Replaces the launch part
+ * of sapporo::startGravCalc / evaluate_gravity
+ * (lib/src/sapporohostclass.cpp:586-703, 1442-1602). */
+int sapb_force(sapb_dev *d, int nj, int ni, double eps2, double ti, int flags);
+
+/* Waits for the last sapb_force and returns its pinned result records
+ * (SAPB_RES_STRIDE doubles per i).  Replaces the blocking readback of
+ * sapporo::getGravResults (lib/src/sapporohostclass.cpp:705-802, 949-966). */
+int sapb_results(sapb_dev *d, const double **results, int *ni);
+
+/* Copies the neighbour counts and lists of the last force call to the host.
+ * counts: ni ints; lists: ni*SAPB_NGB_PB ints (may be NULL).  Replaces
+ * fetch_ngb_list_from_device (lib/src/sapporohostclass.cpp:1149-1162). */
+int sapb_ngb_fetch(sapb_dev *d, int *counts, int *lists, int ni);
+
+/* Device-resident variants for callers that keep i-data on the GPU
+ * (no host copies; `i_dev`, `res_dev` are device pointers with the record
+ * layouts above; asynchronous on the device stream). */
+int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
+                      double *res_dev, int *ngb_count_dev, int *ngb_list_dev);
+
+/* FP64 state of j[first, first+n), 24 doubles per j:
+ *   x[3] mass v[3] eps acc[3] jerk[3] px[3] pv[3] pa[3] id
+ * where px/pv/pa are the FP64 prediction to ti (predict != 0) or the raw
+ * state (predict == 0).  Synchronous.  Backs retrieve_predicted_j_particle
+ * and retrieve_j_particle_state (lib/src/sapporohostclass.cpp:969-1147). */
+int sapb_read_j(sapb_dev *d, int first, int n, double ti, int predict, double *out);
+
+/* Launch-shape override for the force kernel: threads per i (1,2,4,8,16,32),
+ * i per thread (1,2) and j slices (>= 1).  Zeros restore the built-in
+ * planner.  Replaces the compile-time NTHREADS / NBLOCKS_PER_MULTI tables
+ * (lib/include/defines.h:13-122). */
+int sapb_set_launch(sapb_dev *d, int tpi, int ip, int nslices);
+int sapb_get_plan(sapb_dev *d, int ni, int nj, int *tpi, int *ip, int *nslices);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,387 @@
+"""Python mirror of the Sapporo2 B200 library interfaces.
+
+The product is the native library ``sapporo2_b200/lib/libsapporo_b200.so``
+(CUDA kernels for sm_100a + the C++ ``sapporo`` class + the GRAPE-6 ``g6_*``
+exports).  This module binds it with ctypes so that tests, the benchmark and
+Python integrators can drive it:
+
+* :class:`Sapporo` -- the ``sapporo`` C++ class (reference
+  lib/include/sapporohostclass.h:125-175) through ``include/sapporo_c.h``;
+* :class:`G6` -- the GRAPE-6 functions (reference
+  lib/interfaces/sapporoG6lib.cpp), called exactly as a C/Fortran caller
+  would;
+* :class:`Device` -- the lower sapb_* C ABI (``include/sapporo_b200.h``),
+  including device-resident force calls for callers that keep data on the GPU.
+
+There is no CPU fallback: if the library is missing or no sm_100 GPU is
+present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+GRAPE5, FOURTH, SIXTH = 0, 1, 2
+FLOAT, DOUBLESINGLE, DOUBLE = 0, 1, 2
+NGB_PB = 256
+NPIPES = 16384
+RES_STRIDE = 12
+F_PREDICT = 1
+F_NGB_LIST = 2
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "lib" / "libsapporo_b200.so"
+
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+class SapporoError(RuntimeError):
+    pass
+
+
+def _opt(ptr_type):
+    """ndpointer that also accepts None."""
+
+    class _P(ptr_type):  # type: ignore[misc, valid-type]
+        @classmethod
+        def from_param(cls, obj):
+            if obj is None:
+                return None
+            return ptr_type.from_param(obj)
+
+    return _P
+
+
+_dpo = _opt(_dp)
+_ipo = _opt(_ip)
+
+# (name, restype, argtypes)
+_SIGS = [
+    ("sapb_version", C.c_char_p, []),
+    ("sapb_error_string", C.c_char_p, [C.c_int]),
+    ("sapb_last_error", C.c_char_p, [C.c_void_p]),
+    ("sapb_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("sapb_open", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("sapb_close", C.c_int, [C.c_void_p]),
+    ("sapb_info", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 5),
+    ("sapb_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("sapb_reserve_j", C.c_int, [C.c_void_p, C.c_int]),
+    ("sapb_j_stage", C.c_void_p, [C.c_void_p, C.c_int]),
+    ("sapb_j_stage_stride", C.c_int, [C.c_void_p]),
+    ("sapb_push_j", C.c_int, [C.c_void_p, C.c_int]),
+    ("sapb_predict", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("sapb_i_stage", C.c_void_p, [C.c_void_p, C.c_int]),
+    ("sapb_i_stage_stride", C.c_int, [C.c_void_p]),
+    ("sapb_force", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
+    ("sapb_results", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
+    ("sapb_ngb_fetch", C.c_int, [C.c_void_p, _ipo, _ipo, C.c_int]),
+    ("sapb_force_device", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double,
+                                    C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("sapb_read_j", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _dp]),
+    ("sapb_set_launch", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    ("sapb_get_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 3),
+    # class binding
+    ("sapporo_c_new", C.c_void_p, []),
+    ("sapporo_c_delete", None, [C.c_void_p]),
+    ("sapporo_c_open", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    ("sapporo_c_close", C.c_int, [C.c_void_p]),
+    ("sapporo_c_get_n_pipes", C.c_int, [C.c_void_p]),
+    ("sapporo_c_set_time", C.c_int, [C.c_void_p, C.c_double]),
+    ("sapporo_c_set_no_time", C.c_int, [C.c_void_p]),
+    ("sapporo_c_set_j_particles", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _dpo, _dp, _dp, _dp,
+                                            _dp, _dp, _dpo, _dpo, _dpo]),
+    ("sapporo_c_start", C.c_int, [C.c_void_p, C.c_int, C.c_int, _ip, _dp, _dp, _dpo, C.c_double,
+                                  _dpo]),
+    ("sapporo_c_results", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dpo, _dpo, _dp, _ipo,
+                                    _dpo, C.c_int]),
+    ("sapporo_c_force_prediction", C.c_int, [C.c_void_p, C.c_int]),
+    ("sapporo_c_read_ngb_list", C.c_int, [C.c_void_p]),
+    ("sapporo_c_get_ngb_list", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), _ip]),
+    ("sapporo_c_retrieve_predicted", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("sapporo_c_retrieve_state", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("sapporo_c_last_status", C.c_int, [C.c_void_p]),
+    ("sapporo_c_device", C.c_void_p, [C.c_void_p]),
+    # GRAPE-6
+    ("g6_open_", C.c_int, [C.POINTER(C.c_int)]),
+    ("g6_open_special", C.c_int, [C.c_int, C.POINTER(C.c_int)]),
+    ("g6_close_", C.c_int, [C.POINTER(C.c_int)]),
+    ("g6_npipes_", C.c_int, []),
+    ("g6_set_tunit_", C.c_int, [C.POINTER(C.c_double)]),
+    ("g6_set_xunit_", C.c_int, [C.POINTER(C.c_double)]),
+    ("g6_set_ti_", C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("g6_set_j_particle_", C.c_int, [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)] * 3
+     + [_dp] * 5),
+    ("g6calc_firsthalf_", None, [C.POINTER(C.c_int)] * 3 + [_ip, _dp, _dp, _dp, _dp, _dp,
+                                                             C.POINTER(C.c_double), _dp]),
+    ("g6calc_lasthalf_", C.c_int, [C.POINTER(C.c_int)] * 3 + [_ip, _dp, _dp,
+                                                              C.POINTER(C.c_double), _dp, _dp,
+                                                              _dp, _dp]),
+    ("g6calc_lasthalf2_", C.c_int, [C.POINTER(C.c_int)] * 3 + [_ip, _dp, _dp,
+                                                               C.POINTER(C.c_double), _dp, _dp,
+                                                               _dp, _dp, _ip]),
+    ("g6_initialize_jp_buffer_", C.c_int, [C.POINTER(C.c_int)] * 2),
+    ("g6_flush_jp_buffer_", C.c_int, [C.POINTER(C.c_int)]),
+    ("g6_reset_", C.c_int, [C.POINTER(C.c_int)]),
+    ("g6_reset_fofpga_", C.c_int, [C.POINTER(C.c_int)]),
+    ("g6_read_neighbour_list_", C.c_int, [C.POINTER(C.c_int)]),
+    ("g6_get_neighbour_list_", C.c_int, [C.POINTER(C.c_int)] * 4 + [_ip]),
+]
+
+
+def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Loads libsapporo_b200.so (built by ``python -m sapporo2_b200.build``)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise SapporoError(f"{p} is missing; build it with `python -m sapporo2_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, res, args in _SIGS:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return [s[0] for s in _SIGS]
+
+
+def _check(rc: int, what: str, handle=None) -> int:
+    if rc < 0:
+        lib = load_library()
+        detail = lib.sapb_last_error(handle).decode() if handle is not None else \
+            lib.sapb_last_error(None).decode()
+        raise SapporoError(f"{what}: {lib.sapb_error_string(rc).decode()} ({detail})")
+    return rc
+
+
+def device_count() -> int:
+    lib = load_library()
+    n = C.c_int(0)
+    lib.sapb_device_count(C.byref(n))
+    return n.value
+
+
+def _f64(a, shape=None):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Sapporo:
+    """The ``sapporo`` class (C++), one GPU.  Method names follow the
+    reference; array arguments are numpy arrays ([n, 3] for vectors)."""
+
+    def __init__(self, device: int = 0, order: int = FOURTH, precision: int = DOUBLESINGLE):
+        self.lib = load_library()
+        self.h = self.lib.sapporo_c_new()
+        if not self.h:
+            raise SapporoError("allocation failed")
+        self.order = order
+        self.precision = precision
+        _check(self.lib.sapporo_c_open(self.h, device, order, precision), "open")
+        self.dev = self.lib.sapporo_c_device(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.sapporo_c_close(self.h)
+            self.lib.sapporo_c_delete(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_n_pipes(self) -> int:
+        return self.lib.sapporo_c_get_n_pipes(self.h)
+
+    def set_time(self, t: float):
+        _check(self.lib.sapporo_c_set_time(self.h, float(t)), "set_time")
+
+    def set_no_time(self):
+        _check(self.lib.sapporo_c_set_no_time(self.h), "set_no_time")
+
+    def set_j_particles(self, address, id, t, mass, x, v, a, jrk, snp=None, crk=None, eps=None):
+        address = _i32(address)
+        n = len(address)
+        _check(self.lib.sapporo_c_set_j_particles(
+            self.h, n, address, _i32(id), _f64(t), _f64(mass), _f64(x, (n, 3)), _f64(v, (n, 3)),
+            _f64(a, (n, 3)), _f64(jrk, (n, 3)), _f64(snp, (n, 3)) if snp is not None else None,
+            _f64(crk, (n, 3)) if crk is not None else None, _f64(eps)), "set_j_particle",
+            self.dev)
+
+    def start(self, nj, id, xi, vi, ai=None, eps2=0.0, h2=None):
+        id = _i32(id)
+        ni = len(id)
+        _check(self.lib.sapporo_c_start(self.h, int(nj), ni, id, _f64(xi, (ni, 3)),
+                                        _f64(vi, (ni, 3)),
+                                        _f64(ai, (ni, 3)) if ai is not None else None,
+                                        float(eps2), _f64(h2)), "startGravCalc", self.dev)
+        self._ni = ni
+
+    def results(self, nj, ni=None, ngb=True) -> dict:
+        ni = self._ni if ni is None else ni
+        acc = np.zeros((ni, 3))
+        jrk = np.zeros((ni, 3))
+        snp = np.zeros((ni, 3))
+        pot = np.zeros(ni)
+        nnb = np.zeros(ni, dtype=np.int32)
+        dsmin = np.full(ni, np.nan)
+        _check(self.lib.sapporo_c_results(self.h, int(nj), ni, acc, jrk, snp, pot, nnb, dsmin,
+                                          1 if ngb else 0), "getGravResults", self.dev)
+        return {"acc": acc, "jrk": jrk, "snp": snp, "pot": pot, "nnb": nnb, "ds2min": dsmin}
+
+    def force_prediction(self, nj):
+        _check(self.lib.sapporo_c_force_prediction(self.h, int(nj)), "forcePrediction", self.dev)
+
+    def read_ngb_list(self) -> int:
+        return self.lib.sapporo_c_read_ngb_list(self.h)
+
+    def get_ngb_list(self, ipipe: int, maxlength: int = NGB_PB):
+        buf = np.zeros(max(maxlength, 1), dtype=np.int32)
+        n = C.c_int(0)
+        ovf = self.lib.sapporo_c_get_ngb_list(self.h, int(ipipe), int(maxlength), C.byref(n), buf)
+        return ovf, n.value, buf[:min(n.value, maxlength, NGB_PB)].copy()
+
+    def retrieve_predicted(self, addr: int) -> dict:
+        o = np.zeros(12)
+        _check(self.lib.sapporo_c_retrieve_predicted(self.h, int(addr), o), "retrieve", self.dev)
+        return {"mass": o[0], "id": o[1], "eps2": o[2], "pos": o[3:6].copy(),
+                "vel": o[6:9].copy(), "acc": o[9:12].copy()}
+
+    def retrieve_state(self, addr: int) -> dict:
+        o = np.zeros(24)
+        _check(self.lib.sapporo_c_retrieve_state(self.h, int(addr), o), "retrieve", self.dev)
+        keys = ["pos", "vel", "acc", "jrk", "ppos", "pvel", "pacc"]
+        d = {"mass": o[0], "id": o[1], "eps2": o[2]}
+        for k, name in enumerate(keys):
+            d[name] = o[3 + 3 * k: 6 + 3 * k].copy()
+        return d
+
+    # lower level
+    def set_launch(self, tpi=0, ip=0, nslices=0):
+        _check(self.lib.sapb_set_launch(self.dev, tpi, ip, nslices), "set_launch", self.dev)
+
+    def plan(self, ni, nj):
+        t, i, s = C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.sapb_get_plan(self.dev, ni, nj, C.byref(t), C.byref(i), C.byref(s)),
+               "plan", self.dev)
+        return t.value, i.value, s.value
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(self.lib.sapb_set_stream(self.dev, C.c_void_p(stream_ptr or 0)), "set_stream",
+               self.dev)
+
+
+class G6:
+    """The GRAPE-6 interface, called through its C ABI (one process-wide
+    instance, as in the reference)."""
+
+    def __init__(self):
+        self.lib = load_library()
+
+    @staticmethod
+    def _i(v):
+        return C.byref(C.c_int(int(v)))
+
+    @staticmethod
+    def _d(v):
+        return C.byref(C.c_double(float(v)))
+
+    def open(self, cluster=0):
+        return self.lib.g6_open_(self._i(cluster))
+
+    def open_special(self, devices=(0,)):
+        arr = (C.c_int * len(devices))(*devices)
+        return self.lib.g6_open_special(len(devices), arr)
+
+    def close(self, cluster=0):
+        return self.lib.g6_close_(self._i(cluster))
+
+    def npipes(self):
+        return self.lib.g6_npipes_()
+
+    def set_ti(self, ti, cluster=0):
+        return self.lib.g6_set_ti_(self._i(cluster), self._d(ti))
+
+    def set_j_particle(self, address, index, tj, dtj, mass, k18, j6, a2, v, x, cluster=0):
+        return self.lib.g6_set_j_particle_(self._i(cluster), self._i(address), self._i(index),
+                                           self._d(tj), self._d(dtj), self._d(mass),
+                                           _f64(k18), _f64(j6), _f64(a2), _f64(v), _f64(x))
+
+    def calc_firsthalf(self, nj, index, xi, vi, aold, j6old, phiold, eps2, h2, cluster=0):
+        index = _i32(index)
+        ni = len(index)
+        self.lib.g6calc_firsthalf_(self._i(cluster), self._i(nj), self._i(ni), index,
+                                   _f64(xi, (ni, 3)), _f64(vi, (ni, 3)), _f64(aold, (ni, 3)),
+                                   _f64(j6old, (ni, 3)), _f64(phiold), self._d(eps2), _f64(h2))
+
+    def calc_lasthalf(self, nj, index, xi, vi, eps2, h2, cluster=0):
+        index = _i32(index)
+        ni = len(index)
+        acc, jrk, pot = np.zeros((ni, 3)), np.zeros((ni, 3)), np.zeros(ni)
+        rc = self.lib.g6calc_lasthalf_(self._i(cluster), self._i(nj), self._i(ni), index,
+                                       _f64(xi, (ni, 3)), _f64(vi, (ni, 3)), self._d(eps2),
+                                       _f64(h2), acc, jrk, pot)
+        return rc, acc, jrk, pot
+
+    def calc_lasthalf2(self, nj, index, xi, vi, eps2, h2, cluster=0):
+        index = _i32(index)
+        ni = len(index)
+        acc, jrk, pot = np.zeros((ni, 3)), np.zeros((ni, 3)), np.zeros(ni)
+        inn = np.zeros(ni, dtype=np.int32)
+        rc = self.lib.g6calc_lasthalf2_(self._i(cluster), self._i(nj), self._i(ni), index,
+                                        _f64(xi, (ni, 3)), _f64(vi, (ni, 3)), self._d(eps2),
+                                        _f64(h2), acc, jrk, pot, inn)
+        return rc, acc, jrk, pot, inn
+
+    def read_neighbour_list(self, cluster=0):
+        return self.lib.g6_read_neighbour_list_(self._i(cluster))
+
+    def get_neighbour_list(self, ipipe, maxlength=NGB_PB, cluster=0):
+        buf = np.zeros(max(maxlength, 1), dtype=np.int32)
+        n = C.c_int(0)
+        ovf = self.lib.g6_get_neighbour_list_(self._i(cluster), self._i(ipipe),
+                                              self._i(maxlength), C.byref(n), buf)
+        return ovf, n.value, buf[:min(n.value, maxlength, NGB_PB)].copy()
+
+
+def pack_i_records(order, x, v, h2, ids, a=None) -> np.ndarray:
+    """i records in the layout of sapb_i_stage (for device-resident calls)."""
+    n = len(ids)
+    stride = 12 if order >= SIXTH else 8
+    rec = np.zeros((n, stride))
+    rec[:, 0:3] = x
+    rec[:, 3] = 0.0 if h2 is None else h2
+    rec[:, 4:7] = v
+    idw = np.zeros(n, dtype=np.int64)
+    idw[:] = np.asarray(ids, dtype=np.int64) & 0xFFFFFFFF
+    rec[:, 7] = idw.view(np.float64)
+    if order >= SIXTH and a is not None:
+        rec[:, 8:11] = a
+    return rec

@@ -1,0 +1,106 @@
+"""Builds libsapporo_b200.so in-tree (sapporo2_b200/lib/) for sm_100a.
+
+    python -m sapporo2_b200.build [--force] [--jobs N]
+
+CUDA sources are compiled with nvcc for sm_100a only (the library refuses
+other devices at open time); C++ host sources with the system g++.  The CUDA
+runtime is linked statically, so the .so needs only the driver at run time.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = PKG / "_build"
+LIBDIR = PKG / "lib"
+LIBNAME = "libsapporo_b200.so"
+
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+HOST_CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + [
+    "-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX,
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-Wall",
+    f"-I{INCLUDE}", f"-I{CSRC}",
+]
+CXX_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CSRC}",
+             f"-I{CUDA_HOME / 'include'}"]
+
+CU_SOURCES = ["sapb_kernels.cu", "sapb_capi.cu"]
+CXX_SOURCES = ["sapporohostclass.cpp", "sapporoG6lib.cpp", "sapporo_cbind.cpp"]
+
+
+def _headers() -> list[Path]:
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
+
+
+def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in [src, *deps])
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} {cmd[-1]}")
+
+
+def library_path() -> Path:
+    return LIBDIR / LIBNAME
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
+    if not Path(NVCC).exists():
+        raise RuntimeError(f"nvcc not found at {NVCC}")
+    BUILD.mkdir(exist_ok=True)
+    LIBDIR.mkdir(exist_ok=True)
+    deps = _headers()
+    steps = []
+    objs = []
+    for s in CU_SOURCES:
+        src, obj = CSRC / s, BUILD / (s + ".o")
+        objs.append(obj)
+        if force or _stale(obj, src, deps):
+            steps.append([NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+    for s in CXX_SOURCES:
+        src, obj = CSRC / s, BUILD / (s + ".o")
+        objs.append(obj)
+        if force or _stale(obj, src, deps):
+            steps.append([HOST_CXX, *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
+    with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        list(ex.map(_run, steps))
+    lib = library_path()
+    if force or steps or not lib.exists():
+        tmp = lib.with_suffix(".so.tmp")
+        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-ccbin", HOST_CXX,
+              "-o", str(tmp), *map(str, objs)])
+        shutil.move(str(tmp), str(lib))
+    if verbose:
+        print(f"built {lib}")
+    return lib
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=None)
+    a = ap.parse_args()
+    build(force=a.force, jobs=a.jobs, verbose=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,595 @@
+// C ABI over the device code: device state, staging, launch planning.
+// Declared in include/sapporo_b200.h.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+
+#include "../../include/sapporo_b200.h"
+#include "sapb_launch.h"
+
+using namespace sapb;
+
+struct sapb_dev {
+  int device = 0;
+  int order = FOURTH;
+  int prec = DOUBLESINGLE;
+  int n_pipes = SAPB_NPIPES;
+  int num_sms = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+
+  // j state
+  int cap = 0;
+  JState js{};
+  void *pred = nullptr;
+  double *jpool = nullptr;  // one allocation holding the FP64 planes
+  int *jid = nullptr;
+
+  // j staging
+  double *stage_h = nullptr;
+  double *stage_d = nullptr;
+  int stage_cap = 0;
+
+  // i records, results
+  double *irec_h = nullptr, *irec_d = nullptr;
+  int i_cap = 0;
+  double *res_h = nullptr, *res_d = nullptr;
+  int *ngb_count_d = nullptr, *ngb_list_d = nullptr;
+  double *part_d = nullptr;
+  size_t part_cap = 0;  // doubles
+  int *status_d = nullptr, *status_h = nullptr;
+  int last_ni = 0;
+  bool pending = false;
+
+  // launch overrides (0 = planner)
+  int tpi = 0, ip = 0, nslices = 0;
+
+  char err[512] = {0};
+};
+
+static char g_err[512];
+
+static int fail(sapb_dev *d, int code, const char *fmt, ...) {
+  char *buf = d ? d->err : g_err;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(d, call)                                                                       \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail((d), SAPB_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),       \
+                  __FILE__, __LINE__);                                                    \
+  } while (0)
+
+static size_t pred_bytes_per_j(int order, int prec) {
+  return prec == DOUBLE ? 32u * pred_fields64(order) : 16u * pred_fields(order);
+}
+static int nplanes(int order) {  // FP64 planes: t m eps + 3*(x v a j) [+ 3*(s c)]
+  return 3 + 12 + (order >= SIXTH ? 6 : 0);
+}
+
+static void free_j(sapb_dev *d) {
+  if (d->jpool) cudaFree(d->jpool);
+  if (d->jid) cudaFree(d->jid);
+  if (d->pred) cudaFree(d->pred);
+  d->jpool = nullptr;
+  d->jid = nullptr;
+  d->pred = nullptr;
+  d->cap = 0;
+}
+
+static void bind_planes(JState &js, double *pool, int *id, int cap, int order) {
+  double *p = pool;
+  js.t = p; p += cap;
+  js.m = p; p += cap;
+  js.eps = p; p += cap;
+  for (int d = 0; d < 3; d++) { js.x[d] = p; p += cap; }
+  for (int d = 0; d < 3; d++) { js.v[d] = p; p += cap; }
+  for (int d = 0; d < 3; d++) { js.a[d] = p; p += cap; }
+  for (int d = 0; d < 3; d++) { js.j[d] = p; p += cap; }
+  for (int d = 0; d < 3; d++) {
+    js.s[d] = order >= SIXTH ? p : nullptr;
+    if (order >= SIXTH) p += cap;
+  }
+  for (int d = 0; d < 3; d++) {
+    js.c[d] = order >= SIXTH ? p : nullptr;
+    if (order >= SIXTH) p += cap;
+  }
+  js.id = id;
+}
+
+// Grows j storage to new_cap, copying the first old cap entries of every
+// plane and of the predicted records.
+static int grow_j(sapb_dev *d, int new_cap) {
+  if (new_cap <= d->cap) return SAPB_OK;
+  const int np = nplanes(d->order);
+  double *pool = nullptr;
+  int *id = nullptr;
+  void *pred = nullptr;
+  const size_t pb = pred_bytes_per_j(d->order, d->prec);
+  if (cudaMalloc(&pool, sizeof(double) * np * (size_t)new_cap) != cudaSuccess ||
+      cudaMalloc(&id, sizeof(int) * (size_t)new_cap) != cudaSuccess ||
+      cudaMalloc(&pred, pb * (size_t)new_cap) != cudaSuccess) {
+    cudaGetLastError();
+    if (pool) cudaFree(pool);
+    if (id) cudaFree(id);
+    if (pred) cudaFree(pred);
+    return fail(d, SAPB_ENOMEM, "cannot allocate j storage for %d particles", new_cap);
+  }
+  CK(d, cudaMemsetAsync(pool, 0, sizeof(double) * np * (size_t)new_cap, d->stream));
+  CK(d, cudaMemsetAsync(id, 0, sizeof(int) * (size_t)new_cap, d->stream));
+  CK(d, cudaMemsetAsync(pred, 0, pb * (size_t)new_cap, d->stream));
+  if (d->cap > 0) {
+    for (int k = 0; k < np; k++)
+      CK(d, cudaMemcpyAsync(pool + (size_t)k * new_cap, d->jpool + (size_t)k * d->cap,
+                            sizeof(double) * d->cap, cudaMemcpyDeviceToDevice, d->stream));
+    CK(d, cudaMemcpyAsync(id, d->jid, sizeof(int) * d->cap, cudaMemcpyDeviceToDevice, d->stream));
+    CK(d, cudaMemcpyAsync(pred, d->pred, pb * d->cap, cudaMemcpyDeviceToDevice, d->stream));
+    CK(d, cudaStreamSynchronize(d->stream));
+  }
+  free_j(d);
+  d->jpool = pool;
+  d->jid = id;
+  d->pred = pred;
+  d->cap = new_cap;
+  bind_planes(d->js, pool, id, new_cap, d->order);
+  return SAPB_OK;
+}
+
+static int ensure_i(sapb_dev *d, int ni) {
+  if (ni <= d->i_cap) return SAPB_OK;
+  const int cap = std::max(ni, d->n_pipes);
+  const int is = i_stride(d->order);
+  double *ih = nullptr, *id = nullptr, *rh = nullptr, *rd = nullptr;
+  int *cnt = nullptr, *lst = nullptr;
+  bool ok = cudaHostAlloc(&ih, sizeof(double) * is * (size_t)cap, cudaHostAllocDefault) ==
+                cudaSuccess &&
+            cudaMalloc(&id, sizeof(double) * is * (size_t)cap) == cudaSuccess &&
+            cudaHostAlloc(&rh, sizeof(double) * kResStride * (size_t)cap,
+                          cudaHostAllocDefault) == cudaSuccess &&
+            cudaMalloc(&rd, sizeof(double) * kResStride * (size_t)cap) == cudaSuccess &&
+            cudaMalloc(&cnt, sizeof(int) * (size_t)cap) == cudaSuccess &&
+            cudaMalloc(&lst, sizeof(int) * kNgbPB * (size_t)cap) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    if (ih) cudaFreeHost(ih);
+    if (rh) cudaFreeHost(rh);
+    if (id) cudaFree(id);
+    if (rd) cudaFree(rd);
+    if (cnt) cudaFree(cnt);
+    if (lst) cudaFree(lst);
+    return fail(d, SAPB_ENOMEM, "cannot allocate i buffers for %d particles", cap);
+  }
+  if (d->irec_h) {
+    memcpy(ih, d->irec_h, sizeof(double) * is * (size_t)d->i_cap);
+    cudaFreeHost(d->irec_h);
+  }
+  if (d->res_h) cudaFreeHost(d->res_h);
+  if (d->irec_d) cudaFree(d->irec_d);
+  if (d->res_d) cudaFree(d->res_d);
+  if (d->ngb_count_d) cudaFree(d->ngb_count_d);
+  if (d->ngb_list_d) cudaFree(d->ngb_list_d);
+  d->irec_h = ih;
+  d->irec_d = id;
+  d->res_h = rh;
+  d->res_d = rd;
+  d->ngb_count_d = cnt;
+  d->ngb_list_d = lst;
+  d->i_cap = cap;
+  CK(d, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)cap, d->stream));
+  return SAPB_OK;
+}
+
+static int ensure_part(sapb_dev *d, size_t doubles) {
+  if (doubles <= d->part_cap) return SAPB_OK;
+  if (d->part_d) cudaFree(d->part_d);
+  d->part_d = nullptr;
+  d->part_cap = 0;
+  const size_t want = doubles + doubles / 4;
+  if (cudaMalloc(&d->part_d, sizeof(double) * want) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(d, SAPB_ENOMEM, "cannot allocate %zu bytes of partial sums", sizeof(double) * want);
+  }
+  d->part_cap = want;
+  return SAPB_OK;
+}
+
+// ---------------------------------------------------------------------
+// Launch planner: threads-per-i, i per thread and the number of j slices.
+// Scores every shape by the fraction of i slots that carry a particle
+// times how well the grid fills `target` resident blocks.
+// ---------------------------------------------------------------------
+struct Plan {
+  int tpi, ip, ns, i_tiles, slice_tiles;
+};
+
+static int blocks_per_sm(int order, int prec, int ip) {
+  if (prec == DOUBLE) return ip == 2 ? 3 : 4;
+  if (order >= SIXTH) return ip == 2 ? 3 : 5;
+  return ip == 2 ? 3 : 6;
+}
+
+static Plan make_plan(const sapb_dev *d, int ni, int nj) {
+  const int tj = force_tile_j();
+  const int ntiles = std::max(1, (nj + tj - 1) / tj);
+  static const int shapes[][2] = {{1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
+  Plan best{1, 2, 1, 1, ntiles};
+  double best_score = -1.0;
+  for (auto &sh : shapes) {
+    const int tpi = d->tpi ? d->tpi : sh[0];
+    const int ip = d->ip ? d->ip : sh[1];
+    const int ti = force_tile_i(tpi, ip);
+    const int i_tiles = (ni + ti - 1) / ti;
+    const long target = 2L * d->num_sms * blocks_per_sm(d->order, d->prec, ip);
+    int ns = d->nslices;
+    if (!ns) {
+      const int max_ns = std::max(1, ntiles / 4);  // keep >= 4 tiles per slice
+      ns = (int)std::min<long>(max_ns, (target + i_tiles - 1) / i_tiles);
+      ns = std::max(ns, 1);
+    }
+    const int st = (ntiles + ns - 1) / ns;
+    ns = (ntiles + st - 1) / st;  // every slice non-empty
+    const double fill = std::min(1.0, (double)i_tiles * ns / (double)target);
+    const double used = (double)ni / ((double)i_tiles * ti);
+    const double score = fill * used;
+    if (score > best_score + 1e-9) {
+      best_score = score;
+      best = Plan{tpi, ip, ns, i_tiles, st};
+    }
+    if (d->tpi) break;  // fixed shape
+  }
+  return best;
+}
+
+// ---------------------------------------------------------------------
+extern "C" {
+
+const char *sapb_version(void) { return "sapporo-b200 0.1 (sm_100a)"; }
+
+const char *sapb_error_string(int code) {
+  switch (code) {
+    case SAPB_OK: return "ok";
+    case SAPB_ECUDA: return "CUDA runtime error";
+    case SAPB_EINVAL: return "invalid argument";
+    case SAPB_ENOMEM: return "out of memory";
+    case SAPB_ETIMEOUT: return "device wait timed out";
+    case SAPB_ENODEV: return "no CUDA device";
+    default: return "unknown error";
+  }
+}
+
+const char *sapb_last_error(const sapb_dev *d) { return d ? d->err : g_err; }
+
+int sapb_device_count(int *count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    return fail(nullptr, SAPB_ENODEV, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+  }
+  *count = n;
+  return SAPB_OK;
+}
+
+int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
+              int nj_reserve) {
+  if (!out) return fail(nullptr, SAPB_EINVAL, "null handle pointer");
+  *out = nullptr;
+  if (order != FOURTH && order != SIXTH)
+    return fail(nullptr, SAPB_EINVAL, "order %d not supported (4th=1, 6th=2)", order);
+  if (precision != DOUBLESINGLE && precision != DOUBLE)
+    return fail(nullptr, SAPB_EINVAL, "precision %d not supported (DS=1, DOUBLE=2)", precision);
+  int ndev = 0;
+  if (sapb_device_count(&ndev) != SAPB_OK || ndev == 0)
+    return fail(nullptr, SAPB_ENODEV, "no CUDA device available");
+  if (device < 0 || device >= ndev)
+    return fail(nullptr, SAPB_EINVAL, "device %d out of range (%d devices)", device, ndev);
+  sapb_dev *d = new (std::nothrow) sapb_dev();
+  if (!d) return fail(nullptr, SAPB_ENOMEM, "host allocation failed");
+  d->device = device;
+  d->order = order;
+  d->prec = precision;
+  d->n_pipes = n_pipes > 0 ? n_pipes : SAPB_NPIPES;
+  int rc = SAPB_OK;
+  do {
+    if (cudaSetDevice(device) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "cudaSetDevice(%d)", device); break; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "cudaGetDeviceProperties"); break; }
+    d->num_sms = prop.multiProcessorCount;
+    if (prop.major < 10) {
+      rc = fail(d, SAPB_ENODEV, "device %d is sm_%d%d; this build targets sm_100a", device,
+                prop.major, prop.minor);
+      break;
+    }
+    if (cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "stream"); break; }
+    d->stream = d->own_stream;
+    if (cudaEventCreateWithFlags(&d->done, cudaEventDisableTiming) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "event"); break; }
+    if (cudaMalloc(&d->status_d, sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc(&d->status_h, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+      rc = fail(d, SAPB_ENOMEM, "status word");
+      break;
+    }
+    *d->status_h = 0;
+    if (cudaMemsetAsync(d->status_d, 0, sizeof(int), d->stream) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "memset"); break; }
+    rc = grow_j(d, nj_reserve > 0 ? nj_reserve : 16384);
+    if (rc) break;
+    rc = ensure_i(d, d->n_pipes);
+    if (rc) break;
+    if (cudaStreamSynchronize(d->stream) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "sync"); break; }
+  } while (0);
+  if (rc != SAPB_OK) {
+    snprintf(g_err, sizeof g_err, "%s", d->err);
+    sapb_close(d);
+    cudaGetLastError();
+    return rc;
+  }
+  *out = d;
+  return SAPB_OK;
+}
+
+int sapb_close(sapb_dev *d) {
+  if (!d) return SAPB_OK;
+  cudaSetDevice(d->device);
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  free_j(d);
+  if (d->stage_h) cudaFreeHost(d->stage_h);
+  if (d->stage_d) cudaFree(d->stage_d);
+  if (d->irec_h) cudaFreeHost(d->irec_h);
+  if (d->irec_d) cudaFree(d->irec_d);
+  if (d->res_h) cudaFreeHost(d->res_h);
+  if (d->res_d) cudaFree(d->res_d);
+  if (d->ngb_count_d) cudaFree(d->ngb_count_d);
+  if (d->ngb_list_d) cudaFree(d->ngb_list_d);
+  if (d->part_d) cudaFree(d->part_d);
+  if (d->status_d) cudaFree(d->status_d);
+  if (d->status_h) cudaFreeHost(d->status_h);
+  if (d->done) cudaEventDestroy(d->done);
+  if (d->own_stream) cudaStreamDestroy(d->own_stream);
+  delete d;
+  return SAPB_OK;
+}
+
+int sapb_info(const sapb_dev *d, int *order, int *precision, int *n_pipes, int *j_capacity,
+              int *num_sms) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  if (order) *order = d->order;
+  if (precision) *precision = d->prec;
+  if (n_pipes) *n_pipes = d->n_pipes;
+  if (j_capacity) *j_capacity = d->cap;
+  if (num_sms) *num_sms = d->num_sms;
+  return SAPB_OK;
+}
+
+int sapb_set_stream(sapb_dev *d, void *stream) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  CK(d, cudaStreamSynchronize(d->stream));
+  d->stream = stream ? (cudaStream_t)stream : d->own_stream;
+  return SAPB_OK;
+}
+
+int sapb_reserve_j(sapb_dev *d, int nj_capacity) {
+  if (!d || nj_capacity < 0) return fail(d, SAPB_EINVAL, "bad capacity");
+  CK(d, cudaSetDevice(d->device));
+  return grow_j(d, nj_capacity);
+}
+
+int sapb_j_stage_stride(const sapb_dev *d) { return d ? stage_stride(d->order) : 0; }
+int sapb_i_stage_stride(const sapb_dev *d) { return d ? i_stride(d->order) : 0; }
+
+double *sapb_j_stage(sapb_dev *d, int n) {
+  if (!d || n < 0) return nullptr;
+  if (n <= d->stage_cap) return d->stage_h;
+  const int ss = stage_stride(d->order);
+  const int cap = std::max(n, d->stage_cap + d->stage_cap / 2 + 1024);
+  double *h = nullptr, *dd = nullptr;
+  cudaSetDevice(d->device);
+  if (cudaHostAlloc(&h, sizeof(double) * ss * (size_t)cap, cudaHostAllocDefault) != cudaSuccess ||
+      cudaMalloc(&dd, sizeof(double) * ss * (size_t)cap) != cudaSuccess) {
+    cudaGetLastError();
+    if (h) cudaFreeHost(h);
+    fail(d, SAPB_ENOMEM, "cannot allocate staging for %d j records", cap);
+    return nullptr;
+  }
+  if (d->stage_h) {
+    cudaStreamSynchronize(d->stream);  // a pending push may still read the old buffer
+    memcpy(h, d->stage_h, sizeof(double) * ss * (size_t)d->stage_cap);
+    cudaFreeHost(d->stage_h);
+    cudaFree(d->stage_d);
+  }
+  d->stage_h = h;
+  d->stage_d = dd;
+  d->stage_cap = cap;
+  return h;
+}
+
+int sapb_push_j(sapb_dev *d, int n) {
+  if (!d || n < 0 || n > d->stage_cap) return fail(d, SAPB_EINVAL, "push of %d records", n);
+  if (n == 0) return SAPB_OK;
+  CK(d, cudaSetDevice(d->device));
+  // grow the j store to cover the highest staged address
+  int maxaddr = -1;
+  const int ss = stage_stride(d->order);
+  for (int k = 0; k < n; k++) {
+    int addr;
+    memcpy(&addr, d->stage_h + (size_t)k * ss, sizeof(int));
+    if (addr < 0) return fail(d, SAPB_EINVAL, "negative j address %d", addr);
+    maxaddr = std::max(maxaddr, addr);
+  }
+  if (maxaddr >= d->cap) {
+    int rc = grow_j(d, std::max(maxaddr + 1, (int)(d->cap * 1.1) + 1));
+    if (rc) return rc;
+  }
+  CK(d, cudaMemcpyAsync(d->stage_d, d->stage_h, sizeof(double) * ss * (size_t)n,
+                        cudaMemcpyHostToDevice, d->stream));
+  CK(d, launch_scatter(d->order, d->prec, d->stage_d, n, d->cap, d->js, d->pred, d->status_d,
+                       d->stream));
+  // the host may overwrite the staging buffer once the copy has been consumed
+  CK(d, cudaStreamSynchronize(d->stream));
+  return SAPB_OK;
+}
+
+int sapb_predict(sapb_dev *d, int nj, double ti) {
+  if (!d || nj < 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "predict of %d j (capacity %d)", nj, d ? d->cap : 0);
+  CK(d, cudaSetDevice(d->device));
+  CK(d, launch_predict(d->order, d->prec, nj, ti, d->js, d->pred, d->stream));
+  return SAPB_OK;
+}
+
+double *sapb_i_stage(sapb_dev *d, int ni) {
+  if (!d || ni < 0) return nullptr;
+  cudaSetDevice(d->device);
+  if (d->pending) {  // do not hand out a buffer an in-flight copy still reads
+    cudaEventSynchronize(d->done);
+  }
+  if (ensure_i(d, ni) != SAPB_OK) return nullptr;
+  return d->irec_h;
+}
+
+static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
+                     double *res_dev, int *cnt_dev, int *list_dev) {
+  if (nj <= 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "nj = %d (capacity %d)", nj, d->cap);
+  const Plan P = make_plan(d, ni, nj);
+  const bool list = (flags & SAPB_F_NGB_LIST) != 0;
+  if (list) CK(d, cudaMemsetAsync(cnt_dev, 0, sizeof(int) * (size_t)ni, d->stream));
+  ForceArgs A{};
+  A.pred = d->pred;
+  A.nj = nj;
+  A.irec = i_dev;
+  A.ni = ni;
+  A.eps2 = eps2;
+  A.nslices = P.ns;
+  A.slice_tiles = P.slice_tiles;
+  A.i_tiles = P.i_tiles;
+  A.do_list = list ? 1 : 0;
+  A.ngb_count = cnt_dev;
+  A.ngb_list = list_dev;
+  A.status = d->status_d;
+  if (P.ns > 1) {
+    int rc = ensure_part(d, (size_t)P.ns * ni * kResStride);
+    if (rc) return rc;
+    A.out = d->part_d;
+    A.write_partials = 1;
+  } else {
+    A.out = res_dev;
+    A.write_partials = 0;
+  }
+  CK(d, launch_force(d->order, d->prec, A, P.tpi, P.ip, d->stream));
+  if (P.ns > 1) {
+    ReduceArgs R{d->part_d, P.ns, ni, res_dev, cnt_dev};
+    CK(d, launch_reduce(R, d->stream));
+  }
+  return SAPB_OK;
+}
+
+int sapb_force(sapb_dev *d, int nj, int ni, double eps2, double ti, int flags) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  if (ni < 0 || ni > d->i_cap) return fail(d, SAPB_EINVAL, "ni = %d (staged capacity %d)", ni, d->i_cap);
+  CK(d, cudaSetDevice(d->device));
+  if (flags & SAPB_F_PREDICT) {
+    int rc = sapb_predict(d, nj, ti);
+    if (rc) return rc;
+  }
+  d->last_ni = ni;
+  if (ni == 0) return SAPB_OK;
+  const int is = i_stride(d->order);
+  CK(d, cudaMemcpyAsync(d->irec_d, d->irec_h, sizeof(double) * is * (size_t)ni,
+                        cudaMemcpyHostToDevice, d->stream));
+  int rc = run_force(d, nj, ni, d->irec_d, eps2, flags, d->res_d, d->ngb_count_d, d->ngb_list_d);
+  if (rc) return rc;
+  CK(d, cudaMemcpyAsync(d->res_h, d->res_d, sizeof(double) * kResStride * (size_t)ni,
+                        cudaMemcpyDeviceToHost, d->stream));
+  CK(d, cudaMemcpyAsync(d->status_h, d->status_d, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+  CK(d, cudaEventRecord(d->done, d->stream));
+  d->pending = true;
+  return SAPB_OK;
+}
+
+int sapb_results(sapb_dev *d, const double **results, int *ni) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  CK(d, cudaSetDevice(d->device));
+  if (d->pending) {
+    CK(d, cudaEventSynchronize(d->done));
+    d->pending = false;
+  }
+  if (results) *results = d->res_h;
+  if (ni) *ni = d->last_ni;
+  if (*d->status_h) {
+    const int s = *d->status_h;
+    *d->status_h = 0;
+    cudaMemsetAsync(d->status_d, 0, sizeof(int), d->stream);
+    if (s & kErrWaitTimeout) return fail(d, SAPB_ETIMEOUT, "force kernel: bounded wait for a j tile timed out");
+    return fail(d, SAPB_EINVAL, "device reported status 0x%x", s);
+  }
+  return SAPB_OK;
+}
+
+int sapb_ngb_fetch(sapb_dev *d, int *counts, int *lists, int ni) {
+  if (!d || ni < 0 || ni > d->i_cap) return fail(d, SAPB_EINVAL, "bad ni %d", ni);
+  CK(d, cudaSetDevice(d->device));
+  if (ni == 0) return SAPB_OK;
+  if (counts)
+    CK(d, cudaMemcpyAsync(counts, d->ngb_count_d, sizeof(int) * (size_t)ni,
+                          cudaMemcpyDeviceToHost, d->stream));
+  if (lists)
+    CK(d, cudaMemcpyAsync(lists, d->ngb_list_d, sizeof(int) * kNgbPB * (size_t)ni,
+                          cudaMemcpyDeviceToHost, d->stream));
+  CK(d, cudaStreamSynchronize(d->stream));
+  return SAPB_OK;
+}
+
+int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
+                      double *res_dev, int *ngb_count_dev, int *ngb_list_dev) {
+  if (!d || !i_dev || !res_dev || ni < 0) return fail(d, SAPB_EINVAL, "bad arguments");
+  if ((flags & SAPB_F_NGB_LIST) && (!ngb_count_dev || !ngb_list_dev))
+    return fail(d, SAPB_EINVAL, "neighbour lists requested without buffers");
+  CK(d, cudaSetDevice(d->device));
+  if (ni == 0) return SAPB_OK;
+  return run_force(d, nj, ni, i_dev, eps2, flags, res_dev, ngb_count_dev, ngb_list_dev);
+}
+
+int sapb_set_launch(sapb_dev *d, int tpi, int ip, int nslices) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  const bool ok_tpi = tpi == 0 || tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8 ||
+                      ((tpi == 16 || tpi == 32) && ip == 1);
+  if (!ok_tpi || (ip != 0 && ip != 1 && ip != 2) || nslices < 0 || (tpi && !ip))
+    return fail(d, SAPB_EINVAL, "unsupported launch shape tpi=%d ip=%d slices=%d", tpi, ip, nslices);
+  d->tpi = tpi;
+  d->ip = ip;
+  d->nslices = nslices;
+  return SAPB_OK;
+}
+
+int sapb_get_plan(sapb_dev *d, int ni, int nj, int *tpi, int *ip, int *nslices) {
+  if (!d || ni <= 0 || nj <= 0) return fail(d, SAPB_EINVAL, "bad sizes");
+  const Plan P = make_plan(d, ni, nj);
+  if (tpi) *tpi = P.tpi;
+  if (ip) *ip = P.ip;
+  if (nslices) *nslices = P.ns;
+  return SAPB_OK;
+}
+
+int sapb_read_j(sapb_dev *d, int first, int n, double ti, int predict, double *out) {
+  if (!d || first < 0 || n < 0 || first + n > d->cap || (n > 0 && !out))
+    return fail(d, SAPB_EINVAL, "read of j[%d, %d) (capacity %d)", first, first + n, d ? d->cap : 0);
+  if (n == 0) return SAPB_OK;
+  CK(d, cudaSetDevice(d->device));
+  const size_t need = (size_t)n * 24;
+  int rc = ensure_part(d, need);
+  if (rc) return rc;
+  CK(d, launch_readj(d->order, first, n, ti, predict, d->js, d->part_d, d->stream));
+  CK(d, cudaMemcpyAsync(out, d->part_d, sizeof(double) * need, cudaMemcpyDeviceToHost, d->stream));
+  CK(d, cudaStreamSynchronize(d->stream));
+  return SAPB_OK;
+}
+
+}  // extern "C"

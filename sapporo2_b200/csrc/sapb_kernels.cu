@@ -1,0 +1,690 @@
+// Device kernels of the direct-summation hot path and their host launchers.
+// See sapb_kernels.cuh for the list and sapb_internal.cuh for the layouts.
+#include <float.h>
+
+#include "sapb_kernels.cuh"
+#include "sapb_launch.h"
+
+namespace sapb {
+
+// ========================================================================
+// Scatter: staged j -> FP64 state + unpredicted force record.
+// The unpredicted copy is what the force uses when no prediction is asked
+// for (reference: dev_copy_particles seeds Ppos/Pvel/Pacc,
+// kernels.cu:281-297).
+// ========================================================================
+template <int ORDER, int PREC>
+__device__ __forceinline__ void store_record(void *pred, int k, double px, double py, double pz,
+                                             double m, int id, double vx, double vy, double vz,
+                                             double ax, double ay, double az) {
+  if (PREC == DOUBLE) {
+    double4 *r = reinterpret_cast<double4 *>(pred) + (size_t)k * pred_fields64(ORDER);
+    r[0] = make_double4(px, py, pz, m);
+    r[1] = make_double4(vx, vy, vz, __hiloint2double(0, id));
+    if (ORDER >= SIXTH) r[2] = make_double4(ax, ay, az, 0.0);
+  } else {
+    // Double-single split of the position: hi = (float)x, lo = (float)(x - hi)
+    // (the DSX assignment of kernels.cu:163-167).
+    const float hx = (float)px, hy = (float)py, hz = (float)pz;
+    const float lx = (float)(px - (double)hx), ly = (float)(py - (double)hy),
+                lz = (float)(pz - (double)hz);
+    float4 *r = reinterpret_cast<float4 *>(pred) + (size_t)k * pred_fields(ORDER);
+    r[0] = make_float4(hx, hy, hz, (float)m);
+    r[1] = make_float4(lx, ly, lz, __int_as_float(id));
+    r[2] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
+    if (ORDER >= SIXTH) r[3] = make_float4((float)ax, (float)ay, (float)az, 0.f);
+  }
+}
+
+template <int ORDER, int PREC>
+__global__ void __launch_bounds__(256) scatter_kernel(const double *__restrict__ stage, int n,
+                                                      int cap, JState js, void *pred,
+                                                      int *status) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double *r = stage + (size_t)k * stage_stride(ORDER);
+  const int addr = __double2loint(r[0]);
+  const int id = __double2hiint(r[0]);
+  if (addr < 0 || addr >= cap) {
+    atomicOr(status, kErrBadConfig);
+    return;
+  }
+  js.t[addr] = r[1];
+  js.m[addr] = r[2];
+  js.eps[addr] = r[15];
+  js.id[addr] = id;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    js.x[d][addr] = r[3 + d];
+    js.v[d][addr] = r[6 + d];
+    js.a[d][addr] = r[9 + d];
+    js.j[d][addr] = r[12 + d];
+    if (ORDER >= SIXTH) {
+      js.s[d][addr] = r[16 + d];
+      js.c[d][addr] = r[19 + d];
+    }
+  }
+  store_record<ORDER, PREC>(pred, addr, r[3], r[4], r[5], r[2], id, r[6], r[7], r[8], r[9], r[10],
+                            r[11]);
+}
+
+// ========================================================================
+// Predictor: FP64 Taylor series in the Horner form of kernels.cu:331-383
+// (4th order drops snap/crackle, which the reference does by dt4 = dt5 = 0).
+// Reads the FP64 structure-of-arrays state with one coalesced 8-byte load
+// per component and writes the force record of each j.
+// ========================================================================
+template <int ORDER>
+__device__ __forceinline__ void taylor(const JState &js, int k, double ti, double p[3],
+                                       double v[3], double a[3]) {
+  const double dt = ti - __ldg(js.t + k);
+  const double dt2 = (1. / 2.) * dt;
+  const double dt3 = (1. / 3.) * dt;
+  const double dt4 = (1. / 4.) * dt;
+  const double dt5 = (1. / 5.) * dt;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double x = __ldg(js.x[d] + k), vv = __ldg(js.v[d] + k);
+    const double aa = __ldg(js.a[d] + k), jj = __ldg(js.j[d] + k);
+    if (ORDER >= SIXTH) {
+      const double ss = __ldg(js.s[d] + k), cc = __ldg(js.c[d] + k);
+      p[d] = x + dt * (vv + dt2 * (aa + dt3 * (jj + dt4 * (ss + dt5 * (cc)))));
+      v[d] = vv + dt * (aa + dt2 * (jj + dt3 * (ss + dt4 * (cc))));
+      a[d] = aa + dt * (jj + dt2 * (ss + dt3 * (cc)));
+    } else {
+      p[d] = x + dt * (vv + dt2 * (aa + dt3 * (jj)));
+      v[d] = vv + dt * (aa + dt2 * (jj));
+      a[d] = aa;
+    }
+  }
+}
+
+template <int ORDER, int PREC>
+__global__ void __launch_bounds__(256) predict_kernel(int nj, double ti, JState js, void *pred) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nj) return;
+  double p[3], v[3], a[3];
+  taylor<ORDER>(js, k, ti, p, v, a);
+  store_record<ORDER, PREC>(pred, k, p[0], p[1], p[2], __ldg(js.m + k), __ldg(js.id + k), v[0],
+                            v[1], v[2], a[0], a[1], a[2]);
+}
+
+// Readback of j[first, first+n): raw FP64 state and its FP64 prediction to
+// ti (or the raw state again when predict == 0), 24 doubles per j:
+//   x[3] m v[3] eps a[3] jerk[3] px[3] pv[3] pa[3] id
+template <int ORDER>
+__global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti, int predict,
+                                                    JState js, double *out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int k = first + q;
+  double p[3], v[3], a[3];
+  if (predict) {
+    taylor<ORDER>(js, k, ti, p, v, a);
+  } else {
+    for (int d = 0; d < 3; d++) {
+      p[d] = js.x[d][k];
+      v[d] = js.v[d][k];
+      a[d] = js.a[d][k];
+    }
+  }
+  double *o = out + (size_t)q * 24;
+  for (int d = 0; d < 3; d++) {
+    o[d] = js.x[d][k];
+    o[4 + d] = js.v[d][k];
+    o[8 + d] = js.a[d][k];
+    o[11 + d] = js.j[d][k];
+    o[14 + d] = p[d];
+    o[17 + d] = v[d];
+    o[20 + d] = a[d];
+  }
+  o[3] = js.m[k];
+  o[7] = js.eps[k];
+  o[23] = (double)js.id[k];
+}
+
+// ========================================================================
+// Force kernel.
+//
+// Block = 128 threads laid out as TPI rows x TIT = 128/TPI columns; each
+// thread owns IP i-particles (columns tx, tx+TIT, ...), so a block covers an
+// i-tile of TI = TIT*IP particles.  blockIdx.y selects a j-slice of
+// `slice_tiles` tiles of TJ = 128 records.  Thread 0 streams the slice's
+// tiles into a 3-stage shared-memory ring with cp.async.bulk and mbarrier
+// completion; row `ty` of the block consumes records ty, ty+TPI, ... of
+// each tile.
+//
+// Mixed precision (DOUBLESINGLE): dr = (xj_hi - xi_hi) + (xj_lo - xi_lo)
+// in FP32 (double-single difference, kernels.cu:169-177), FP32 body with
+// rsqrt on the MUFU pipe, FP32 sums per tile folded into FP64 totals after
+// every tile.  FP64 (DOUBLE): every step in double, rsqrt(double).
+//
+// The self pair (id_i == id_j, kernels.cu:565) is removed by replacing dx
+// with a huge value, which makes ds2 ~ 1e36 (1e300 in FP64): its force
+// underflows to zero and it can be neither nearest neighbour nor listed.
+//
+// Nearest neighbour and neighbour list are found per tile: the pair loop
+// only keeps the tile's minimum ds2; when that minimum is below the current
+// best or below h2, the (rare) rescan recomputes ds2 bit-identically for the
+// tile and emits list entries / the best (ds2, id) key.
+// ========================================================================
+constexpr int kBT = 128;
+constexpr int kTJ = 128;
+constexpr int kNS = 3;
+
+template <int ORDER, int PREC, int TPI, int IP>
+struct FCfg {
+  static constexpr int TIT = kBT / TPI;
+  static constexpr int TI = TIT * IP;
+  static constexpr int FB = PREC == DOUBLE ? 32 : 16;
+  static constexpr int RS = PREC == DOUBLE ? pred_fields64(ORDER) : pred_fields(ORDER);
+  static constexpr int REC = RS * FB;
+  static constexpr int TILE_BYTES = kTJ * REC;
+  static constexpr int RED_BYTES = TPI > 1 ? kBT * IP * kResStride * 8 : 0;
+  static constexpr int BODY = kNS * TILE_BYTES > RED_BYTES ? kNS * TILE_BYTES : RED_BYTES;
+  static constexpr int SMEM = 128 + BODY;
+};
+
+// ---------------- mixed precision pair ----------------
+struct IMix {
+  float xh, yh, zh, xl, yl, zl, vx, vy, vz, ax, ay, az, h2;
+  int id;
+};
+struct AccMix {
+  float ax, ay, az, pot, jx, jy, jz, sx, sy, sz;
+};
+
+__device__ __forceinline__ float ds_sub(float jh, float jl, float ih, float il) {
+  return __fadd_rn(__fsub_rn(jh, ih), __fsub_rn(jl, il));
+}
+// dr and ds2 of one pair, self pair masked; identical in the pair loop and
+// in the rescans (explicitly rounded operations, no contraction freedom).
+__device__ __forceinline__ float pair_dr_mix(const IMix &I, const float4 &r0, const float4 &r1,
+                                             float &dx, float &dy, float &dz) {
+  dx = ds_sub(r0.x, r1.x, I.xh, I.xl);
+  dy = ds_sub(r0.y, r1.y, I.yh, I.yl);
+  dz = ds_sub(r0.z, r1.z, I.zh, I.zl);
+  dx = (__float_as_int(r1.w) == I.id) ? 1.0e18f : dx;
+  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+template <int ORDER>
+__device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const float4 &r1,
+                                         const float4 &r2, const float4 &r3, float eps2,
+                                         AccMix &A, float &tmin) {
+  float dx, dy, dz;
+  const float ds2 = pair_dr_mix(I, r0, r1, dx, dy, dz);
+  tmin = fminf(tmin, ds2);
+  const float inv = rsqrt_mufu(ds2 + eps2);
+  const float inv2 = inv * inv;
+  const float minv = r0.w * inv;
+  const float minv3 = minv * inv2;
+  A.ax = fmaf(minv3, dx, A.ax);
+  A.ay = fmaf(minv3, dy, A.ay);
+  A.az = fmaf(minv3, dz, A.az);
+  A.pot -= minv;
+  const float dvx = r2.x - I.vx, dvy = r2.y - I.vy, dvz = r2.z - I.vz;
+  const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
+  const float m3i2 = -3.0f * inv2;
+  if (ORDER == FOURTH) {
+    // jerk += m/r^3 dv - 3 m/r^5 (dr.dv) dr   (kernels.cu:631-637)
+    const float c = (m3i2 * minv3) * rv;
+    A.jx = fmaf(c, dx, fmaf(minv3, dvx, A.jx));
+    A.jy = fmaf(c, dy, fmaf(minv3, dvy, A.jy));
+    A.jz = fmaf(c, dz, fmaf(minv3, dvz, A.jz));
+  } else {
+    // kernels.cu:642-667 with a3 = -3 alpha, b3 = -3 beta:
+    //   jerk_ij = minv3 (dv + a3 dr)
+    //   snap   += minv3 (da + b3 dr) + 2 a3 jerk_ij
+    const float dax = r3.x - I.ax, day = r3.y - I.ay, daz = r3.z - I.az;
+    const float s = fmaf(dz, daz, fmaf(dy, day, fmaf(dx, dax, fmaf(dvz, dvz, fmaf(dvy, dvy, dvx * dvx)))));
+    const float a3 = m3i2 * rv;
+    const float b3 = fmaf(a3, a3 * (-1.0f / 3.0f), s * m3i2);
+    const float c6 = (a3 + a3) * minv3;
+    const float tx = fmaf(a3, dx, dvx), ty = fmaf(a3, dy, dvy), tz = fmaf(a3, dz, dvz);
+    A.jx = fmaf(minv3, tx, A.jx);
+    A.jy = fmaf(minv3, ty, A.jy);
+    A.jz = fmaf(minv3, tz, A.jz);
+    const float ux = fmaf(b3, dx, dax), uy = fmaf(b3, dy, day), uz = fmaf(b3, dz, daz);
+    A.sx = fmaf(c6, tx, fmaf(minv3, ux, A.sx));
+    A.sy = fmaf(c6, ty, fmaf(minv3, uy, A.sy));
+    A.sz = fmaf(c6, tz, fmaf(minv3, uz, A.sz));
+  }
+}
+
+// ---------------- FP64 pair ----------------
+struct IDp {
+  double x, y, z, vx, vy, vz, ax, ay, az, h2;
+  int id;
+};
+struct AccDp {
+  double ax, ay, az, pot, jx, jy, jz, sx, sy, sz;
+};
+
+__device__ __forceinline__ double pair_dr_dp(const IDp &I, const double4 &r0, const double4 &r1,
+                                             double &dx, double &dy, double &dz) {
+  dx = __dsub_rn(r0.x, I.x);
+  dy = __dsub_rn(r0.y, I.y);
+  dz = __dsub_rn(r0.z, I.z);
+  dx = (__double2loint(r1.w) == I.id) ? 1.0e150 : dx;
+  return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+}
+
+template <int ORDER>
+__device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const double4 &r1,
+                                        const double4 &r2, double eps2, AccDp &A, double &tmin) {
+  double dx, dy, dz;
+  const double ds2 = pair_dr_dp(I, r0, r1, dx, dy, dz);
+  tmin = fmin(tmin, ds2);
+  const double inv = rsqrt(ds2 + eps2);
+  const double minvr1 = r0.w * inv;
+  const double invr2 = inv * inv;
+  const double minvr3 = minvr1 * invr2;
+  A.ax += minvr3 * dx;
+  A.ay += minvr3 * dy;
+  A.az += minvr3 * dz;
+  A.pot += -minvr1;
+  const double dvx = r1.x - I.vx, dvy = r1.y - I.vy, dvz = r1.z - I.vz;
+  const double rv = dx * dvx + dy * dvy + dz * dvz;
+  if (ORDER == FOURTH) {
+    const double drdv = (-3.0) * (minvr3 * invr2) * rv;
+    A.jx += minvr3 * dvx + drdv * dx;
+    A.jy += minvr3 * dvy + drdv * dy;
+    A.jz += minvr3 * dvz + drdv * dz;
+  } else {
+    const double dax = r2.x - I.ax, day = r2.y - I.ay, daz = r2.z - I.az;
+    const double v2 = dvx * dvx + dvy * dvy + dvz * dvz;
+    const double ra = dx * dax + dy * day + dz * daz;
+    double alpha = rv * invr2;
+    double beta = (v2 + ra) * invr2 + alpha * alpha;
+    alpha *= -3.0;
+    const double ex = minvr3 * dvx + alpha * (minvr3 * dx);
+    const double ey = minvr3 * dvy + alpha * (minvr3 * dy);
+    const double ez = minvr3 * dvz + alpha * (minvr3 * dz);
+    alpha *= 2.0;
+    beta *= -3.0;
+    A.sx += minvr3 * dax + alpha * ex + beta * (minvr3 * dx);
+    A.sy += minvr3 * day + alpha * ey + beta * (minvr3 * dy);
+    A.sz += minvr3 * daz + alpha * ez + beta * (minvr3 * dz);
+    A.jx += ex;
+    A.jy += ey;
+    A.jz += ez;
+  }
+}
+
+// Per-i running state kept across tiles.
+struct NNState {
+  unsigned long long key;  // best (ds2, id)
+  float best;              // ds2 part of key (float), -1 for padding i
+};
+
+__device__ __forceinline__ void list_push(int *cnt, int *list, int gi, int idj) {
+  const int pos = atomicAdd(cnt + gi, 1);
+  if (pos < kNgbPB) list[(size_t)gi * kNgbPB + pos] = idj;
+}
+
+template <int ORDER, int PREC, int TPI, int IP>
+__global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
+  using C = FCfg<ORDER, PREC, TPI, IP>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  unsigned char *tiles = smem + 128;
+
+  const int tid = threadIdx.x;
+  const int tx = tid % C::TIT;
+  const int ty = tid / C::TIT;
+  const int itile = blockIdx.x;
+  const int slice = blockIdx.y;
+  const int istr = i_stride(ORDER);
+
+  // ---- i-particles of this thread ----
+  int gi[IP];
+  bool valid[IP];
+  IMix Im[IP];
+  IDp Id[IP];
+  NNState nn[IP];
+#pragma unroll
+  for (int p = 0; p < IP; p++) {
+    gi[p] = itile * C::TI + p * C::TIT + tx;
+    valid[p] = gi[p] < A.ni;
+    const double *r = A.irec + (size_t)(valid[p] ? gi[p] : 0) * istr;
+    const double x = r[0], y = r[1], z = r[2], h2 = r[3];
+    const double vx = r[4], vy = r[5], vz = r[6];
+    const int id = __double2loint(r[7]);
+    double ax = 0, ay = 0, az = 0;
+    if (ORDER >= SIXTH) {
+      ax = r[8];
+      ay = r[9];
+      az = r[10];
+    }
+    if (PREC == DOUBLE) {
+      Id[p] = IDp{x, y, z, vx, vy, vz, ax, ay, az, valid[p] ? h2 : -1.0, id};
+    } else {
+      const float hx = (float)x, hy = (float)y, hz = (float)z;
+      Im[p] = IMix{hx, hy, hz, (float)(x - (double)hx), (float)(y - (double)hy),
+                   (float)(z - (double)hz), (float)vx, (float)vy, (float)vz, (float)ax,
+                   (float)ay, (float)az, valid[p] ? (float)h2 : -1.0f, id};
+    }
+    nn[p].key = nn_key(kNoNgbDs2, -1);
+    nn[p].best = valid[p] ? kNoNgbDs2 : -1.0f;
+  }
+
+  // ---- j range of this slice ----
+  const int ntiles_all = (A.nj + kTJ - 1) / kTJ;
+  const int t0 = slice * A.slice_tiles;
+  const int t1 = min(t0 + A.slice_tiles, ntiles_all);
+  const int nt = max(t1 - t0, 0);
+  const unsigned char *pred = reinterpret_cast<const unsigned char *>(A.pred);
+
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < kNS; s++) mbar_init(&bars[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  auto issue = [&](int it) {
+    const int tile = t0 + it;
+    const int cnt = min(kTJ, A.nj - tile * kTJ);
+    const uint32_t bytes = (uint32_t)(cnt * C::REC);
+    uint64_t *bar = &bars[it % kNS];
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(tiles + (it % kNS) * C::TILE_BYTES, pred + (size_t)tile * kTJ * C::REC, bytes, bar);
+  };
+  if (tid == 0) {
+    for (int s = 0; s < kNS && s < nt; s++) issue(s);
+  }
+
+  AccDp D[IP];
+#pragma unroll
+  for (int p = 0; p < IP; p++) D[p] = AccDp{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const float eps2f = (float)A.eps2;
+  bool broken = false;
+
+  for (int it = 0; it < nt; it++) {
+    if (!broken && !mbar_wait_bounded(&bars[it % kNS], (uint32_t)((it / kNS) & 1))) {
+      broken = true;
+      atomicOr(A.status, kErrWaitTimeout);
+    }
+    const int tile = t0 + it;
+    const int cnt = min(kTJ, A.nj - tile * kTJ);
+    const unsigned char *buf = tiles + (it % kNS) * C::TILE_BYTES;
+
+    if (PREC == DOUBLE) {
+      const double4 *rec = reinterpret_cast<const double4 *>(buf);
+      double tmin[IP];
+#pragma unroll
+      for (int p = 0; p < IP; p++) tmin[p] = DBL_MAX;
+#pragma unroll 2
+      for (int k = ty; k < cnt; k += TPI) {
+        const double4 r0 = rec[k * C::RS + 0];
+        const double4 r1 = rec[k * C::RS + 1];
+        const double4 r2 = ORDER >= SIXTH ? rec[k * C::RS + 2] : r1;
+#pragma unroll
+        for (int p = 0; p < IP; p++) pair_dp<ORDER>(Id[p], r0, r1, r2, A.eps2, D[p], tmin[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < IP; p++) {
+        const bool want_list = A.do_list && tmin[p] < Id[p].h2;
+        const bool want_nn = (float)tmin[p] <= nn[p].best;
+        if (want_list || want_nn) {
+          unsigned long long key = nn[p].key;
+          for (int k = ty; k < cnt; k += TPI) {
+            double dx, dy, dz;
+            const double4 r0 = rec[k * C::RS + 0];
+            const double4 r1 = rec[k * C::RS + 1];
+            const double ds2 = pair_dr_dp(Id[p], r0, r1, dx, dy, dz);
+            const int idj = __double2loint(r1.w);
+            if (want_list && ds2 < Id[p].h2) list_push(A.ngb_count, A.ngb_list, gi[p], idj);
+            const float f2 = (float)ds2;
+            if (want_nn && f2 < kNoNgbDs2) key = min(key, nn_key(f2, idj));
+          }
+          nn[p].key = key;
+          nn[p].best = __uint_as_float((unsigned int)(key >> 32));
+        }
+      }
+    } else {
+      const float4 *rec = reinterpret_cast<const float4 *>(buf);
+      AccMix P[IP];
+      float tmin[IP];
+#pragma unroll
+      for (int p = 0; p < IP; p++) {
+        P[p] = AccMix{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        tmin[p] = FLT_MAX;
+      }
+#pragma unroll 2
+      for (int k = ty; k < cnt; k += TPI) {
+        const float4 r0 = rec[k * C::RS + 0];
+        const float4 r1 = rec[k * C::RS + 1];
+        const float4 r2 = rec[k * C::RS + 2];
+        const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+#pragma unroll
+        for (int p = 0; p < IP; p++) pair_mix<ORDER>(Im[p], r0, r1, r2, r3, eps2f, P[p], tmin[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < IP; p++) {
+        D[p].ax += (double)P[p].ax;
+        D[p].ay += (double)P[p].ay;
+        D[p].az += (double)P[p].az;
+        D[p].pot += (double)P[p].pot;
+        D[p].jx += (double)P[p].jx;
+        D[p].jy += (double)P[p].jy;
+        D[p].jz += (double)P[p].jz;
+        if (ORDER >= SIXTH) {
+          D[p].sx += (double)P[p].sx;
+          D[p].sy += (double)P[p].sy;
+          D[p].sz += (double)P[p].sz;
+        }
+        const bool want_list = A.do_list && tmin[p] < Im[p].h2;
+        const bool want_nn = tmin[p] <= nn[p].best;
+        if (want_list || want_nn) {
+          unsigned long long key = nn[p].key;
+          for (int k = ty; k < cnt; k += TPI) {
+            float dx, dy, dz;
+            const float4 r0 = rec[k * C::RS + 0];
+            const float4 r1 = rec[k * C::RS + 1];
+            const float ds2 = pair_dr_mix(Im[p], r0, r1, dx, dy, dz);
+            const int idj = __float_as_int(r1.w);
+            if (want_list && ds2 < Im[p].h2) list_push(A.ngb_count, A.ngb_list, gi[p], idj);
+            if (want_nn && ds2 < kNoNgbDs2) key = min(key, nn_key(ds2, idj));
+          }
+          nn[p].key = key;
+          nn[p].best = __uint_as_float((unsigned int)(key >> 32));
+        }
+      }
+    }
+    __syncthreads();  // every thread is done with this stage's buffer
+    if (tid == 0 && !broken && it + kNS < nt) {
+      fence_proxy_async();
+      issue(it + kNS);
+    }
+  }
+  if (broken && tid == 0) {
+    // Let copies still in flight land before the block's shared memory is
+    // released (bounded; the error is already recorded).
+    for (int it = max(nt - kNS, 0); it < nt; it++)
+      mbar_wait_bounded(&bars[it % kNS], (uint32_t)((it / kNS) & 1));
+  }
+
+  // ---- combine rows (threads-per-i > 1), fixed order ----
+  if (TPI > 1) {
+    __syncthreads();
+    double *red = reinterpret_cast<double *>(tiles);
+#pragma unroll
+    for (int p = 0; p < IP; p++) {
+      double *o = red + ((size_t)(ty * C::TIT + tx) * IP + p) * kResStride;
+      o[0] = D[p].ax; o[1] = D[p].ay; o[2] = D[p].az; o[3] = D[p].pot;
+      o[4] = D[p].jx; o[5] = D[p].jy; o[6] = D[p].jz;
+      o[7] = D[p].sx; o[8] = D[p].sy; o[9] = D[p].sz;
+      o[10] = __longlong_as_double((long long)nn[p].key);
+    }
+    __syncthreads();
+    if (ty != 0) return;
+#pragma unroll
+    for (int p = 0; p < IP; p++) {
+      for (int r = 1; r < TPI; r++) {
+        const double *o = red + ((size_t)(r * C::TIT + tx) * IP + p) * kResStride;
+        D[p].ax += o[0]; D[p].ay += o[1]; D[p].az += o[2]; D[p].pot += o[3];
+        D[p].jx += o[4]; D[p].jy += o[5]; D[p].jz += o[6];
+        D[p].sx += o[7]; D[p].sy += o[8]; D[p].sz += o[9];
+        nn[p].key = min(nn[p].key, (unsigned long long)__double_as_longlong(o[10]));
+      }
+    }
+  }
+
+  // ---- write this block's results ----
+#pragma unroll
+  for (int p = 0; p < IP; p++) {
+    if (!valid[p]) continue;
+    double *o = A.write_partials ? A.out + ((size_t)slice * A.ni + gi[p]) * kResStride
+                                 : A.out + (size_t)gi[p] * kResStride;
+    o[0] = D[p].ax; o[1] = D[p].ay; o[2] = D[p].az; o[3] = D[p].pot;
+    o[4] = D[p].jx; o[5] = D[p].jy; o[6] = D[p].jz;
+    o[7] = D[p].sx; o[8] = D[p].sy; o[9] = D[p].sz;
+    if (A.write_partials) {
+      o[10] = __longlong_as_double((long long)nn[p].key);
+      o[11] = 0.0;
+    } else {
+      o[10] = (double)__uint_as_float((unsigned int)(nn[p].key >> 32));
+      o[11] = (double)(int)(unsigned int)(nn[p].key & 0xffffffffu);
+    }
+  }
+}
+
+// ========================================================================
+// Cross-slice reduction: fixed slice order, so results are bit-stable.
+// ========================================================================
+__global__ void __launch_bounds__(256) reduce_kernel(ReduceArgs R) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R.ni) return;
+  double acc[10];
+#pragma unroll
+  for (int f = 0; f < 10; f++) acc[f] = 0.0;
+  unsigned long long key = nn_key(kNoNgbDs2, -1);
+  for (int s = 0; s < R.nslices; s++) {
+    const double *o = R.part + ((size_t)s * R.ni + i) * kResStride;
+#pragma unroll
+    for (int f = 0; f < 10; f++) acc[f] += o[f];
+    key = min(key, (unsigned long long)__double_as_longlong(o[10]));
+  }
+  double *w = R.out + (size_t)i * kResStride;
+#pragma unroll
+  for (int f = 0; f < 10; f++) w[f] = acc[f];
+  w[10] = (double)__uint_as_float((unsigned int)(key >> 32));
+  w[11] = (double)(int)(unsigned int)(key & 0xffffffffu);
+}
+
+// ========================================================================
+// Host launchers
+// ========================================================================
+template <int ORDER, int PREC>
+static cudaError_t launch_scatter_t(const double *stage, int n, int cap, const JState &js,
+                                   void *pred, int *status, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  scatter_kernel<ORDER, PREC><<<(n + 255) / 256, 256, 0, st>>>(stage, n, cap, js, pred, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(int order, int prec, const double *stage, int n, int cap,
+                           const JState &js, void *pred, int *status, cudaStream_t st) {
+  if (order == FOURTH && prec == DOUBLESINGLE)
+    return launch_scatter_t<FOURTH, DOUBLESINGLE>(stage, n, cap, js, pred, status, st);
+  if (order == FOURTH && prec == DOUBLE)
+    return launch_scatter_t<FOURTH, DOUBLE>(stage, n, cap, js, pred, status, st);
+  if (order == SIXTH && prec == DOUBLESINGLE)
+    return launch_scatter_t<SIXTH, DOUBLESINGLE>(stage, n, cap, js, pred, status, st);
+  if (order == SIXTH && prec == DOUBLE)
+    return launch_scatter_t<SIXTH, DOUBLE>(stage, n, cap, js, pred, status, st);
+  return cudaErrorInvalidValue;
+}
+
+template <int ORDER, int PREC>
+static cudaError_t launch_predict_t(int nj, double ti, const JState &js, void *pred,
+                                    cudaStream_t st) {
+  if (nj <= 0) return cudaSuccess;
+  predict_kernel<ORDER, PREC><<<(nj + 255) / 256, 256, 0, st>>>(nj, ti, js, pred);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_predict(int order, int prec, int nj, double ti, const JState &js, void *pred,
+                           cudaStream_t st) {
+  if (order == FOURTH && prec == DOUBLESINGLE)
+    return launch_predict_t<FOURTH, DOUBLESINGLE>(nj, ti, js, pred, st);
+  if (order == FOURTH && prec == DOUBLE)
+    return launch_predict_t<FOURTH, DOUBLE>(nj, ti, js, pred, st);
+  if (order == SIXTH && prec == DOUBLESINGLE)
+    return launch_predict_t<SIXTH, DOUBLESINGLE>(nj, ti, js, pred, st);
+  if (order == SIXTH && prec == DOUBLE)
+    return launch_predict_t<SIXTH, DOUBLE>(nj, ti, js, pred, st);
+  return cudaErrorInvalidValue;
+}
+
+template <int ORDER, int PREC, int TPI, int IP>
+static cudaError_t launch_force_t(const ForceArgs &A, cudaStream_t st) {
+  using C = FCfg<ORDER, PREC, TPI, IP>;
+  static bool attr_done = false;  // one-time attribute per instantiation
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(force_kernel<ORDER, PREC, TPI, IP>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  dim3 grid(A.i_tiles, A.nslices);
+  force_kernel<ORDER, PREC, TPI, IP><<<grid, kBT, C::SMEM, st>>>(A);
+  return cudaGetLastError();
+}
+
+template <int ORDER, int PREC>
+static cudaError_t launch_force_o(const ForceArgs &A, int tpi, int ip, cudaStream_t st) {
+  if (ip == 2) {
+    switch (tpi) {
+      case 1: return launch_force_t<ORDER, PREC, 1, 2>(A, st);
+      case 2: return launch_force_t<ORDER, PREC, 2, 2>(A, st);
+      case 4: return launch_force_t<ORDER, PREC, 4, 2>(A, st);
+      case 8: return launch_force_t<ORDER, PREC, 8, 2>(A, st);
+      default: break;
+    }
+  } else if (ip == 1) {
+    switch (tpi) {
+      case 1: return launch_force_t<ORDER, PREC, 1, 1>(A, st);
+      case 2: return launch_force_t<ORDER, PREC, 2, 1>(A, st);
+      case 4: return launch_force_t<ORDER, PREC, 4, 1>(A, st);
+      case 8: return launch_force_t<ORDER, PREC, 8, 1>(A, st);
+      case 16: return launch_force_t<ORDER, PREC, 16, 1>(A, st);
+      case 32: return launch_force_t<ORDER, PREC, 32, 1>(A, st);
+      default: break;
+    }
+  }
+  return cudaErrorInvalidConfiguration;
+}
+
+int force_tile_i(int tpi, int ip) { return (kBT / tpi) * ip; }
+int force_tile_j() { return kTJ; }
+
+cudaError_t launch_force(int order, int prec, const ForceArgs &A, int tpi, int ip,
+                         cudaStream_t st) {
+  if (order == FOURTH && prec == DOUBLESINGLE)
+    return launch_force_o<FOURTH, DOUBLESINGLE>(A, tpi, ip, st);
+  if (order == FOURTH && prec == DOUBLE) return launch_force_o<FOURTH, DOUBLE>(A, tpi, ip, st);
+  if (order == SIXTH && prec == DOUBLESINGLE)
+    return launch_force_o<SIXTH, DOUBLESINGLE>(A, tpi, ip, st);
+  if (order == SIXTH && prec == DOUBLE) return launch_force_o<SIXTH, DOUBLE>(A, tpi, ip, st);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_readj(int order, int first, int n, double ti, int predict, const JState &js,
+                         double *out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  if (order >= SIXTH)
+    readj_kernel<SIXTH><<<(n + 255) / 256, 256, 0, st>>>(first, n, ti, predict, js, out);
+  else
+    readj_kernel<FOURTH><<<(n + 255) / 256, 256, 0, st>>>(first, n, ti, predict, js, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const ReduceArgs &R, cudaStream_t st) {
+  if (R.ni <= 0) return cudaSuccess;
+  reduce_kernel<<<(R.ni + 255) / 256, 256, 0, st>>>(R);
+  return cudaGetLastError();
+}
+
+}  // namespace sapb

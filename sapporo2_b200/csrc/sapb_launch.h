@@ -1,0 +1,20 @@
+// Host-side launchers of the device kernels (implemented in sapb_kernels.cu).
+#pragma once
+#include "sapb_internal.cuh"
+
+namespace sapb {
+
+cudaError_t launch_scatter(int order, int prec, const double *stage, int n, int cap,
+                           const JState &js, void *pred, int *status, cudaStream_t st);
+cudaError_t launch_predict(int order, int prec, int nj, double ti, const JState &js, void *pred,
+                           cudaStream_t st);
+cudaError_t launch_force(int order, int prec, const ForceArgs &A, int tpi, int ip,
+                         cudaStream_t st);
+cudaError_t launch_reduce(const ReduceArgs &R, cudaStream_t st);
+cudaError_t launch_readj(int order, int first, int n, double ti, int predict, const JState &js,
+                         double *out, cudaStream_t st);
+
+int force_tile_i(int tpi, int ip);  // i-particles per block
+int force_tile_j();                  // j records per tile
+
+}  // namespace sapb

@@ -1,0 +1,443 @@
+// The `sapporo` class on top of the sapb_* C ABI (one GPU).
+//
+// Behaviour follows lib/src/sapporohostclass.cpp of the reference:
+//   - set_j_particle stages into host memory only; j travel to the GPU at the
+//     next startGravCalc / forcePrediction (:434-558, :669-676);
+//   - set_time makes the next force call predict all j to t_i (:405-415);
+//   - startGravCalc returns after queueing the work, getGravResults blocks
+//     (README.extended:154-171);
+//   - nearest neighbour: taken only when ds2 < 1e10, nnbindex zeroed first,
+//     dsmin_i written only when taken (:722-775);
+//   - neighbour lists: overflow when a count reaches NGB_PB (:804-835),
+//     get_ngb_list copies and sorts (:837-880).
+// Deviations (documented in DESIGN.md): fatal exits become error returns;
+// one GPU is used whatever the device list says; get_ngb_list never copies
+// more than NGB_PB entries and flags overflow when the count reaches NGB_PB.
+#include "../../include/sapporohostclass.h"
+
+#include <cmath>
+#include <cstdint>
+
+#include "../../include/sapporo_b200.h"
+
+namespace {
+bool verbose() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("SAPPORO_VERBOSE");
+    v = (e && *e && *e != '0') ? 1 : 0;
+  }
+  return v == 1;
+}
+void report(const char *what, int rc, sapb_dev *d) {
+  fprintf(stderr, "sapporo: %s failed: %s (%s)\n", what, sapb_error_string(rc), sapb_last_error(d));
+}
+inline void put_int_pair(double *slot, int lo, int hi) {
+  int32_t w[2] = {lo, hi};
+  memcpy(slot, w, sizeof(double));
+}
+}  // namespace
+
+sapporo::sapporo()
+    : dev_(nullptr),
+      n_pipes(NPIPES),
+      nj_max(0),
+      integrationOrder(FOURTH),
+      integrationPrecision(DOUBLESINGLE),
+      EPS2(0.0),
+      t_i(0.0),
+      predict(false),
+      nj_updated(false),
+      predJOnHost(false),
+      nstaged_(0),
+      jcache_n_(0),
+      dev_ni(0),
+      nj_last_(0),
+      ngb_fetched_(false),
+      last_status(0) {}
+
+sapporo::~sapporo() { close(); }
+
+int sapporo::open(std::string kernelFile, int *devices, int nprocs, int order, int precision) {
+  (void)kernelFile;  // kernels are linked into the library
+  if (dev_) close();
+  integrationOrder = order;
+  integrationPrecision = precision;
+  int device = 0;
+  if (nprocs > 0 && devices) device = devices[0];
+  if (nprocs > 1 || nprocs < -1)
+    fprintf(stderr, "sapporo: %d devices requested; this build drives one GPU (device %d)\n",
+            nprocs < 0 ? -nprocs : nprocs, device);
+  const char *np = getenv("SAPPORO_NPIPES");
+  const int pipes = np ? atoi(np) : NPIPES;
+  const int rc = sapb_open(&dev_, device, order, precision, pipes, 16384);
+  last_status = rc;
+  if (rc != SAPB_OK) {
+    report("open", rc, nullptr);
+    dev_ = nullptr;
+    return rc;
+  }
+  sapb_info(dev_, nullptr, nullptr, &n_pipes, nullptr, nullptr);
+  nj_max = 16384;  // lib/src/sapporohostclass.cpp:161-162
+  stage_slot_.assign(nj_max, -1);
+  pred_time_.assign(nj_max, NAN);
+  staged_addr_.clear();
+  nstaged_ = 0;
+  predict = false;
+  nj_updated = false;
+  predJOnHost = false;
+  ngb_fetched_ = false;
+  dev_ni = 0;
+  if (verbose())
+    fprintf(stderr, "sapporo: opened device %d, order %d, precision %d, %d pipes\n", device,
+            order, precision, n_pipes);
+  return 0;
+}
+
+int sapporo::close() {
+  if (dev_) {
+    sapb_close(dev_);
+    dev_ = nullptr;
+  }
+  return 0;
+}
+
+int sapporo::get_n_pipes() { return n_pipes; }
+
+int sapporo::set_time(double time) {
+  t_i = time;
+  predict = true;
+  predJOnHost = false;
+  return 0;
+}
+
+int sapporo::set_no_time() {
+  predict = false;
+  predJOnHost = false;
+  return 0;
+}
+
+void sapporo::increase_jMemory() {
+  // lib/src/sapporohostclass.cpp:560-583 (one device)
+  int temp = (int)(nj_max * 1.1);
+  temp = temp + 1;
+  nj_max = temp;
+  stage_slot_.resize(nj_max, -1);
+  pred_time_.resize(nj_max, NAN);
+  if (dev_) {
+    const int rc = sapb_reserve_j(dev_, nj_max);
+    if (rc) report("reserve_j", rc, dev_);
+  }
+}
+
+int sapporo::set_j_particle(int address, int id, double tj, double dtj, double mass,
+                            double k18[3], double j6[3], double a2[3], double v[3], double x[3],
+                            double snp[3], double crk[3], double eps) {
+  (void)k18;
+  (void)dtj;
+  if (!dev_) return last_status = SAPB_EINVAL;
+  if (address < 0) {
+    fprintf(stderr, "sapporo::set_j_particle: negative address %d\n", address);
+    return last_status = SAPB_EINVAL;
+  }
+  predJOnHost = false;
+  nj_updated = true;
+  if (address >= nj_max) {
+    increase_jMemory();
+    if (address >= nj_max) {
+      // reference: exit(-1) (lib/src/sapporohostclass.cpp:463-466)
+      fprintf(stderr,
+              "sapporo::set_j_particle: address %d beyond %d after growing; send particles in "
+              "address order\n",
+              address, nj_max);
+      return last_status = SAPB_EINVAL;
+    }
+  }
+  int slot = stage_slot_[address];
+  if (slot < 0) {
+    slot = nstaged_++;
+    stage_slot_[address] = slot;
+    staged_addr_.push_back(address);
+  }
+  double *base = sapb_j_stage(dev_, nstaged_);
+  if (!base) {
+    report("j staging", SAPB_ENOMEM, dev_);
+    return last_status = SAPB_ENOMEM;
+  }
+  const int ss = sapb_j_stage_stride(dev_);
+  double *r = base + (size_t)slot * ss;
+  put_int_pair(&r[0], address, id);
+  r[1] = tj;
+  r[2] = mass;
+  for (int d = 0; d < 3; d++) {
+    r[3 + d] = x[d];
+    r[6 + d] = v ? v[d] : 0.0;
+    r[9 + d] = a2 ? a2[d] : 0.0;
+    r[12 + d] = j6 ? j6[d] : 0.0;
+  }
+  r[15] = eps;
+  if (integrationOrder > FOURTH) {
+    for (int d = 0; d < 3; d++) {
+      r[16 + d] = snp ? snp[d] : 0.0;
+      r[19 + d] = crk ? crk[d] : 0.0;
+    }
+  }
+  return 0;
+}
+
+int sapporo::push_staged() {
+  if (!nj_updated || nstaged_ == 0) {
+    nj_updated = false;
+    return 0;
+  }
+  const int rc = sapb_push_j(dev_, nstaged_);
+  for (int a : staged_addr_) {
+    stage_slot_[a] = -1;
+    pred_time_[a] = NAN;
+  }
+  staged_addr_.clear();
+  nstaged_ = 0;
+  nj_updated = false;
+  if (rc) report("push_j", rc, dev_);
+  return rc;
+}
+
+void sapporo::send_j_particles_to_device() {
+  if (dev_) last_status = push_staged();
+}
+
+void sapporo::send_i_particles_to_device(int i) {
+  (void)i;  // i records are uploaded together with the force launch
+}
+
+void sapporo::startGravCalc(int nj, int ni, int id[], double xi[][3], double vi[][3],
+                            double a[][3], double j6old[][3], double phiold[3], double eps2,
+                            double h2[], double eps2_i[]) {
+  (void)j6old;
+  (void)phiold;
+  (void)eps2_i;  // stored by the reference (vel_i.w) but unused by its kernels
+  last_status = 0;
+  if (ni == 0 || nj == 0) return;
+  if (!dev_ || ni < 0 || nj < 0) {
+    last_status = SAPB_EINVAL;
+    return;
+  }
+  EPS2 = eps2;
+  double *rec = sapb_i_stage(dev_, ni);
+  if (!rec) {
+    last_status = SAPB_ENOMEM;
+    report("i staging", last_status, dev_);
+    return;
+  }
+  const int is = sapb_i_stage_stride(dev_);
+  for (int i = 0; i < ni; i++) {
+    double *r = rec + (size_t)i * is;
+    r[0] = xi[i][0];
+    r[1] = xi[i][1];
+    r[2] = xi[i][2];
+    r[3] = h2 ? h2[i] : 0.0;
+    r[4] = vi[i][0];
+    r[5] = vi[i][1];
+    r[6] = vi[i][2];
+    put_int_pair(&r[7], id[i], 0);
+    if (integrationOrder > FOURTH) {
+      r[8] = a[i][0];
+      r[9] = a[i][1];
+      r[10] = a[i][2];
+      r[11] = 0.0;
+    }
+  }
+  int rc = push_staged();
+  if (!rc) {
+    int flags = SAPB_F_NGB_LIST;
+    if (predict) flags |= SAPB_F_PREDICT;
+    rc = sapb_force(dev_, nj, ni, eps2, t_i, flags);
+    if (!rc && predict)
+      for (int k = 0; k < nj && k < (int)pred_time_.size(); k++) pred_time_[k] = t_i;
+  }
+  if (rc) report("startGravCalc", rc, dev_);
+  last_status = rc;
+  dev_ni = ni;
+  nj_last_ = nj;
+  ngb_fetched_ = false;
+  predict = false;
+  predJOnHost = false;
+}
+
+int sapporo::getGravResults(int nj, int ni, int index[], double xi[][3], double vi[][3],
+                            double eps2, double h2[], double acc[][3], double jerk[][3],
+                            double snp[][3], double crk[][3], double pot[], int nnbindex[],
+                            double dsmin_i[], bool ngb) {
+  (void)index; (void)xi; (void)vi; (void)eps2; (void)h2;
+  if (ni == 0 || nj == 0) return 0;
+  for (int i = 0; i < ni; i++) {
+    pot[i] = acc[i][0] = acc[i][1] = acc[i][2] = 0;
+    if (integrationOrder > GRAPE5) jerk[i][0] = jerk[i][1] = jerk[i][2] = 0;
+    if (ngb) nnbindex[i] = 0;
+    if (integrationOrder > FOURTH) {
+      snp[i][0] = snp[i][1] = snp[i][2] = 0;
+      if (crk) crk[i][0] = crk[i][1] = crk[i][2] = 0;
+    }
+  }
+  if (!dev_) return last_status = SAPB_EINVAL;
+  if (last_status) return last_status;
+  const double *res = nullptr;
+  int nres = 0;
+  const int rc = sapb_results(dev_, &res, &nres);
+  if (rc) {
+    report("getGravResults", rc, dev_);
+    return last_status = rc;
+  }
+  const int n = std::min(ni, nres);
+  for (int i = 0; i < n; i++) {
+    const double *r = res + (size_t)i * SAPB_RES_STRIDE;
+    acc[i][0] += r[0];
+    acc[i][1] += r[1];
+    acc[i][2] += r[2];
+    pot[i] += r[3];
+    if (integrationOrder > GRAPE5) {
+      jerk[i][0] += r[4];
+      jerk[i][1] += r[5];
+      jerk[i][2] += r[6];
+      if (ngb) {
+        const double ds = r[10];
+        if (ds < 1.0e10) {  // lib/src/sapporohostclass.cpp:732, 767-774
+          nnbindex[i] = (int)r[11];
+          if (dsmin_i) dsmin_i[i] = ds;
+        }
+      }
+    }
+    if (integrationOrder > FOURTH) {
+      snp[i][0] += r[7];
+      snp[i][1] += r[8];
+      snp[i][2] += r[9];
+    }
+  }
+  return 0;
+}
+
+int sapporo::fetch_ngb_list_from_device(int) {
+  if (!dev_) return 0;
+  ngb_count_h_.resize((size_t)std::max(dev_ni, 1));
+  ngb_list_h_.resize((size_t)std::max(dev_ni, 1) * NGB_PB);
+  const double *res = nullptr;
+  sapb_results(dev_, &res, nullptr);  // the lists belong to the last force call
+  const int rc = sapb_ngb_fetch(dev_, ngb_count_h_.data(), ngb_list_h_.data(), dev_ni);
+  if (rc) {
+    report("ngb fetch", rc, dev_);
+    return 0;
+  }
+  ngb_fetched_ = true;
+  return dev_ni;
+}
+
+int sapporo::read_ngb_list(int cluster_id) {
+  const int ni = fetch_ngb_list_from_device(cluster_id);
+  bool overflow = false;
+  for (int j = 0; j < ni; j++)
+    if (ngb_count_h_[j] >= NGB_PB) overflow = true;
+  return overflow;
+}
+
+int sapporo::get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, int nbl[]) {
+  nblen = 0;
+  if (!ngb_fetched_) fetch_ngb_list_from_device(cluster_id);
+  if (ipipe < 0 || ipipe >= dev_ni || !ngb_fetched_) return 1;
+  const int len = ngb_count_h_[ipipe];
+  const int to_copy = std::max(0, std::min(std::min(len, maxlength), NGB_PB));
+  memcpy(nbl, &ngb_list_h_[(size_t)ipipe * NGB_PB], sizeof(int) * to_copy);
+  nblen = len;
+  const bool overflow = nblen >= maxlength || len >= NGB_PB;
+  std::sort(nbl, nbl + to_copy);
+  if (overflow && verbose())
+    fprintf(stderr, "sapporo::get_ngb_list(..) - overflow for ipipe= %d, ngb= %d\n", ipipe, nblen);
+  return overflow;
+}
+
+void sapporo::forcePrediction(int nj) {
+  if (!dev_) return;
+  int rc = push_staged();
+  if (!rc && predict && nj > 0) {
+    rc = sapb_predict(dev_, nj, t_i);
+    if (!rc)
+      for (int k = 0; k < nj && k < (int)pred_time_.size(); k++) pred_time_[k] = t_i;
+  }
+  if (rc) report("forcePrediction", rc, dev_);
+  last_status = rc;
+  predict = false;
+}
+
+// Reads the FP64 state of every stored j once per modification (like the
+// reference's full readback guarded by predJOnHost), predicted to the time
+// of the most recent prediction; addresses pushed after that prediction or
+// predicted at an older time are handled one by one.
+int sapporo::refresh_jcache(int addr) {
+  if (!dev_) return SAPB_EINVAL;
+  int cap = 0;
+  sapb_info(dev_, nullptr, nullptr, nullptr, &cap, nullptr);
+  if (addr < 0 || addr >= cap) return SAPB_EINVAL;
+  if (!predJOnHost) {
+    push_staged();
+    const int n = std::min(cap, nj_max);
+    jcache_.resize((size_t)n * 24);
+    const int rc = sapb_read_j(dev_, 0, n, t_i, 1, jcache_.data());
+    if (rc) return rc;
+    jcache_n_ = n;
+    predJOnHost = true;
+  }
+  if (addr >= jcache_n_) return SAPB_EINVAL;
+  const double pt = addr < (int)pred_time_.size() ? pred_time_[addr] : NAN;
+  if (std::isnan(pt) || pt != t_i) {
+    double one[24];
+    const int rc = sapb_read_j(dev_, addr, 1, std::isnan(pt) ? 0.0 : pt, std::isnan(pt) ? 0 : 1, one);
+    if (rc) return rc;
+    memcpy(&jcache_[(size_t)addr * 24], one, sizeof one);
+  }
+  return 0;
+}
+
+void sapporo::retrieve_predicted_j_particle(int addr, double &mass, double &id, double &eps2,
+                                            double pos[3], double vel[3], double acc[3]) {
+  last_status = refresh_jcache(addr);
+  if (last_status) {
+    report("retrieve_predicted_j_particle", last_status, dev_);
+    return;
+  }
+  const double *o = &jcache_[(size_t)addr * 24];
+  for (int d = 0; d < 3; d++) {
+    pos[d] = o[14 + d];
+    vel[d] = o[17 + d];
+    if (integrationOrder > FOURTH && acc) acc[d] = o[20 + d];
+  }
+  mass = o[3];
+  eps2 = o[7];
+  id = o[23];
+}
+
+void sapporo::retrieve_j_particle_state(int addr, double &mass, double &id, double &eps2,
+                                        double pos[3], double vel[3], double acc[3],
+                                        double jrk[3], double ppos[3], double pvel[3],
+                                        double pacc[3]) {
+  last_status = refresh_jcache(addr);
+  if (last_status) {
+    report("retrieve_j_particle_state", last_status, dev_);
+    return;
+  }
+  const double *o = &jcache_[(size_t)addr * 24];
+  mass = o[3];
+  for (int d = 0; d < 3; d++) {
+    pos[d] = o[d];
+    if (integrationOrder > GRAPE5) {
+      ppos[d] = o[14 + d];
+      pvel[d] = o[17 + d];
+      vel[d] = o[4 + d];
+      acc[d] = o[8 + d];
+      jrk[d] = o[11 + d];
+    }
+    if (integrationOrder > FOURTH && pacc) pacc[d] = o[20 + d];
+  }
+  if (integrationOrder > GRAPE5) {
+    eps2 = o[7];
+    id = o[23];
+  }
+}
