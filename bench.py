@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Throughput of the direct-summation hot path on B200.
+
+Workload (one "step"): the precision form -- an N = 2^20 Plummer sphere with
+Salpeter masses (0.1-100, slope -2.35, M = 1) and 10 % of the particles in
+circular binaries (a ~ logU(1e-6, 1e-4)), Hermite 6th order; every step
+predicts all j to t_i and evaluates acc/jerk/snap/pot and the nearest
+neighbour on all N i-particles (N^2 interactions).  Inputs are synthetic and
+seeded; the j derivatives come from an FP64 direct summation (the library's
+all-FP64 kernels).
+
+  value   interactions/s of the mixed-precision kernels with all inputs
+          resident in HBM (predictor + force, CUDA events on the launching
+          stream, L2 flushed between steps);
+  e2e     the same metric through the public `sapporo` class with host
+          buffers: j upload, i upload in n_pipes chunks, result download.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (independent replicas)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOPS_4TH, FLOPS_6TH = 38, 60
+METRIC = "interactions/s at N=2^20 mixed vs plain FP64, 1 GPU, acc err<=1e-6; %FP32 peak"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+def build_inputs(n: int, seed: int):
+    from sapporo2_b200 import ic
+    from sapporo2_b200.direct import fp64_direct
+    cfg = ic.make_config("C3", n=n, seed=seed)
+    t0 = time.time()
+    acc, jrk, _ = fp64_direct(1, cfg["x"], cfg["v"], None, cfg["m"], cfg["id"], cfg["eps2"])
+    _, _, snp = fp64_direct(2, cfg["x"], cfg["v"], acc, cfg["m"], cfg["id"], cfg["eps2"])
+    cfg["a"], cfg["j"], cfg["s"] = acc, jrk, snp
+    cfg["c"] = ic.crackle_from(cfg["x"], acc, jrk)
+    cfg["px"], cfg["pv"], cfg["pa"] = ic.predict_fp64(2, cfg["ti"], cfg["t0"], cfg["x"], cfg["v"],
+                                                      acc, jrk, snp, cfg["c"])
+    log(f"[bench] inputs N={n} built in {time.time() - t0:.1f}s")
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "power_w_max": float(max(power)), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+# ---------------------------------------------------------------------------
+LAUNCH = None  # (tpi, ip, slices) override for the force kernel, from --launch
+
+
+def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists=False):
+    """Predictor + force on all N with device-resident inputs.  Returns
+    per-step predictor / force times (ms) and the results."""
+    import sapporo2_b200 as sp
+    n = cfg["n"]
+    s = sp.Sapporo(order=sp.SIXTH, precision=precision)
+    # a dedicated stream: the library and the timing events must share it
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    if LAUNCH and precision == sp.DOUBLESINGLE:
+        s.set_launch(*LAUNCH)
+    s.set_j_particles(np.arange(n), cfg["id"], cfg["t0"], cfg["m"], cfg["x"], cfg["v"], cfg["a"],
+                      cfg["j"], cfg["s"], cfg["c"])
+    s.force_prediction(n)  # uploads and scatters j (no prediction: no set_time yet)
+    rec = sp.pack_i_records(2, cfg["px"], cfg["pv"], cfg["h2"], cfg["id"], cfg["pa"])
+    i_dev = torch.from_numpy(rec).cuda()
+    res = torch.zeros((n, sp.RES_STRIDE), dtype=torch.float64, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda") if lists else None
+    lst = torch.zeros(n * sp.NGB_PB, dtype=torch.int32, device="cuda") if lists else None
+    flags = sp.F_NGB_LIST if lists else 0
+    lib, dev = s.lib, s.dev
+    tpi, ip, ns = s.plan(n, n)
+    pred_ms, force_ms = [], []
+    torch.cuda.synchronize()
+    for it in range(warmup + steps):
+        flush()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        rc = lib.sapb_predict(dev, n, float(cfg["ti"]))
+        e1.record(stream)
+        rc |= lib.sapb_force_device(dev, n, n, i_dev.data_ptr(), float(cfg["eps2"]), flags,
+                                    res.data_ptr(), cnt.data_ptr() if lists else None,
+                                    lst.data_ptr() if lists else None)
+        e2.record(stream)
+        if rc:
+            raise RuntimeError(f"device step failed: {lib.sapb_last_error(dev).decode()}")
+        e2.synchronize()
+        if it >= warmup:
+            pred_ms.append(e0.elapsed_time(e1))
+            force_ms.append(e1.elapsed_time(e2))
+    stream.synchronize()
+    out = res.cpu().numpy()
+    s.close()
+    return {"pred_ms": pred_ms, "force_ms": force_ms, "res": out,
+            "plan": {"tpi": tpi, "ip": ip, "nslices": ns},
+            "launches_per_step": 2 + (1 if ns > 1 else 0)}
+
+
+def e2e_arm(cfg, steps: int):
+    """The public class API with host buffers, n_pipes chunks."""
+    import sapporo2_b200 as sp
+    n = cfg["n"]
+    s = sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE)
+    npipes = s.get_n_pipes()
+    times = []
+    for it in range(steps + 1):  # first pass warms the pinned buffers
+        t0 = time.perf_counter()
+        s.set_j_particles(np.arange(n), cfg["id"], cfg["t0"], cfg["m"], cfg["x"], cfg["v"],
+                          cfg["a"], cfg["j"], cfg["s"], cfg["c"])
+        s.set_time(cfg["ti"])
+        for i0 in range(0, n, npipes):
+            sl = slice(i0, min(n, i0 + npipes))
+            s.start(n, cfg["id"][sl], cfg["px"][sl], cfg["pv"][sl], cfg["pa"][sl], cfg["eps2"],
+                    cfg["h2"][sl])
+            r = s.results(n, ngb=True)
+        t1 = time.perf_counter()
+        if it > 0:
+            times.append(t1 - t0)
+        del r
+    s.close()
+    h2d = n * 22 * 8 + n * 12 * 8
+    d2h = n * 12 * 8
+    return {"s_per_step": float(np.mean(times)), "h2d": h2d, "d2h": d2h, "chunks": -(-n // npipes)}
+
+
+def cpu_baseline_leg(cfg, nsample: int):
+    """FP64 OpenMP direct summation (the project's CPU restatement of the
+    reference's Hermite expressions) on a seeded sample of i against all N j,
+    timed on all host threads.  Also returns the oracle answers for the
+    sample, used as the FP64 truth of the accuracy figures."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(1234)
+    sel = np.sort(rng.choice(cfg["n"], nsample, replace=False)).astype(np.int32)
+    # the oracle predicts the j itself (FP64), exactly as the device does
+    px, pv, pa = O.predict(2, cfg["ti"], cfg["t0"], cfg["x"], cfg["v"], cfg["a"], cfg["j"],
+                           cfg["s"], cfg["c"])
+    threads = O.max_threads()
+    t0 = time.perf_counter()
+    r = O.force_subset(2, sel, cfg["px"], cfg["pv"], cfg["pa"], cfg["h2"], cfg["id"], px, pv, pa,
+                       cfg["m"], cfg["id"], cfg["eps2"], nthreads=threads)
+    dt = time.perf_counter() - t0
+    inter = float(nsample) * cfg["n"]
+    return {"value": inter / dt, "cores": threads, "seconds": dt, "sel": sel, "oracle": r,
+            "interactions": inter}
+
+
+def rel_stats(got, want):
+    e = np.linalg.norm(got - want, axis=1) / np.maximum(np.linalg.norm(want, axis=1), 1e-300)
+    return {"median": float(np.median(e)), "max": float(e.max())}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU implementation of the path is
+    not separable from its host class, so the CPU restatement (oracle port,
+    FP64 OpenMP) of the same Hermite expressions is timed on all host cores,
+    on bounded samples of the same workload."""
+    if rank != 0:
+        return
+    from sapporo2_b200 import ic
+    from oracle import oracle as O
+    n = args.n
+    cfg = ic.make_config("C3", n=n, seed=3)
+    rng = np.random.default_rng(7)
+    z = np.zeros((n, 3))
+    # derivatives do not change the cost of a pair evaluation; use zeros
+    cfg["a"] = cfg["j"] = cfg["s"] = cfg["c"] = z
+    px, pv, pa = O.predict(2, cfg["ti"], cfg["t0"], cfg["x"], cfg["v"], z, z, z, z)
+    threads = O.max_threads()
+    nsample = args.ref_sample
+    times = []
+    for it in range(args.warmup + args.steps):
+        sel = np.sort(rng.choice(n, nsample, replace=False)).astype(np.int32)
+        t0 = time.perf_counter()
+        O.force_subset(2, sel, px, pv, pa, cfg["h2"], cfg["id"], px, pv, pa, cfg["m"], cfg["id"],
+                       cfg["eps2"], nthreads=threads)
+        if it >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    per = float(nsample) * n / np.mean(times)
+    sample = f"{nsample} random i x all {n} j per step (6th order, FP64)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": per, "unit": "interactions/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.mean(times)) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "precision form: Plummer N=2^20, Salpeter masses, 10% binaries, "
+                               "Hermite 6th order", "n": n, "order": 6},
+        "cpu_baseline": {"value": per, "unit": "interactions/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": per, "unit": "interactions/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sapporo_b200")
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=2048)
+    ap.add_argument("--ref-sample", type=int, default=1024)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--launch", default=None,
+                    help="force-kernel shape override tpi,ip,slices (default: planner)")
+    ap.add_argument("--only", choices=["all", "mixed"], default="all",
+                    help="mixed: time only the mixed-precision device arm (profiling runs)")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if args.launch:
+        global LAUNCH
+        LAUNCH = tuple(int(v) for v in args.launch.split(","))
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    os.environ.setdefault("CUDA_VISIBLE_DEVICES_LOCAL", str(local))
+
+    import sapporo2_b200 as sp
+    n = args.n
+    cfg = build_inputs(n, seed=3 + rank)
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush():
+        flush_buf.zero_()
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    mix = device_arm(cfg, sp.DOUBLESINGLE, args.steps, args.warmup, torch, flush)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    step_ms = np.array(mix["pred_ms"]) + np.array(mix["force_ms"])
+    total_ms = float(step_ms.sum())
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    inter_step = float(n) * n
+    value = inter_step * args.steps * world / (total_ms * 1e-3)
+
+    if args.only == "mixed":
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "interactions/s",
+                          "force_ms": float(np.mean(mix["force_ms"])),
+                          "pred_ms": float(np.mean(mix["pred_ms"])), "plan": mix["plan"]}))
+        return
+    f64 = device_arm(cfg, sp.DOUBLE, args.fp64_steps, 1, torch, flush)
+    f64_ms = np.array(f64["pred_ms"]) + np.array(f64["force_ms"])
+    f64_value = inter_step / (f64_ms.mean() * 1e-3)
+
+    e2e = e2e_arm(cfg, args.e2e_steps)
+    e2e_value = inter_step / e2e["s_per_step"]
+    if dist:
+        t = torch.tensor([e2e["s_per_step"]], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = inter_step * world / float(t.item())
+
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    peaks = measured_peaks()
+    props = torch.cuda.get_device_properties(local)
+    nsm = props.multi_processor_count
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = nsm * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s
+    force_ms = float(np.mean(mix["force_ms"]))
+    achieved = FLOPS_6TH * inter_step / (force_ms * 1e-3) / 1e12
+    clk_mhz = clk.get("sm_mhz") or sm_max
+    fp32_peak_run = nsm * 128 * 2 * clk_mhz * 1e6 / 1e12
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    pred_bytes = 224.0  # FP64 inputs 19 doubles read + 9 values written, per j
+    pred_read_write = (19 * 8 + 64)  # bytes actually moved by this predictor (64-B record out)
+    pred_ms = float(np.mean(mix["pred_ms"]))
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 body + ds positions + f64 sums", "data": "synthetic",
+        "config": {"workload": "precision form: Plummer N=2^20, Salpeter masses 0.1-100, 10% "
+                               "circular binaries a~logU(1e-6,1e-4), Hermite 6th order, all i "
+                               "active, NN on, lists off",
+                   "n": n, "order": 6, "precision": "mixed (DS dr, FP32 body, FP64 sums)",
+                   "eps2": cfg["eps2"], "l2": "flushed between steps (256 MB write)",
+                   "launch_plan": mix["plan"], "parallelism": f"replicas x{world}"},
+        "gflops": value * FLOPS_6TH / 1e9,
+        "fp64": {"value": f64_value * world, "unit": "interactions/s",
+                 "ms_per_step": float(f64_ms.mean()), "speedup_mixed_over_fp64": value / world / f64_value},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_note": f"derived: {nsm} SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz "
+                                  "(sm_max_mhz of measured peaks; no FP32 entry there)",
+                     "frac_at_run_clock": achieved / fp32_peak_run,
+                     "flops_per_interaction": FLOPS_6TH, "kernel": "force_kernel<6th,DS>",
+                     "force_ms": force_ms},
+        "roofline_predictor": {"bound": "hbm",
+                               "achieved": pred_bytes * n / (pred_ms * 1e-3) / 1e9,
+                               "peak": hbm, "unit": "GB/s",
+                               "frac": pred_bytes * n / (pred_ms * 1e-3) / 1e9 / hbm,
+                               "bytes_per_j": pred_bytes, "bytes_moved_per_j": pred_read_write,
+                               "pred_ms": pred_ms, "peak_note": "hbm_gbs of measured peaks"},
+        "e2e": {"value": e2e_value, "unit": "interactions/s",
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                "s_per_step": e2e["s_per_step"], "api": "sapporo class, n_pipes chunks",
+                "chunks": e2e["chunks"]},
+        "clocks": clk,
+        "gpu_launches": mix["launches_per_step"] * args.steps,
+    }
+    # accuracy: mixed vs all-FP64 GPU kernel on all N
+    rm, rd = mix["res"], f64["res"]
+    result["accuracy_vs_fp64_gpu"] = {k: rel_stats(rm[:, sl], rd[:, sl]) for k, sl in
+                                      (("acc", slice(0, 3)), ("jrk", slice(4, 7)),
+                                       ("snp", slice(7, 10)))}
+    if not args.no_cpu and world == 1:
+        cb = cpu_baseline_leg(cfg, args.cpu_sample)
+        o, sel = cb["oracle"], cb["sel"]
+        result["cpu_baseline"] = {
+            "value": cb["value"], "unit": "interactions/s", "cores": cb["cores"], "kind": "port",
+            "sample": f"{len(sel)} seeded i x all {n} j, FP64 OpenMP, {cb['seconds']:.1f} s"}
+        acc_m = {}
+        for name, res in (("mixed", rm), ("fp64_gpu", rd)):
+            acc_m[name] = {k: rel_stats(res[sel][:, s3], o[k]) for k, s3 in
+                           (("acc", slice(0, 3)), ("jrk", slice(4, 7)), ("snp", slice(7, 10)))}
+        result["accuracy_vs_fp64_oracle"] = acc_m
+    print(json.dumps(result), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

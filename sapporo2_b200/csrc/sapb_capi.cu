@@ -214,17 +214,21 @@ struct Plan {
 
 static int blocks_per_sm(int order, int prec, int ip) {
   if (prec == DOUBLE) return ip == 2 ? 3 : 4;
-  if (order >= SIXTH) return ip == 2 ? 3 : 5;
-  return ip == 2 ? 3 : 6;
+  (void)order;
+  return ip >= 4 ? 2 : 4;  // mixed: <= 128 registers (ip 1, 2), <= 255 (ip 4)
 }
 
 static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   const int tj = force_tile_j();
   const int ntiles = std::max(1, (nj + tj - 1) / tj);
-  static const int shapes[][2] = {{1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
+  // mixed precision prefers 4 i per thread (two packed FP32x2 chains per j)
+  static const int shapes_mix[][2] = {{1, 4}, {2, 4}, {1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
+  static const int shapes_dp[][2] = {{1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
+  const int nshape = d->prec == DOUBLE ? 6 : 8;
   Plan best{1, 2, 1, 1, ntiles};
   double best_score = -1.0;
-  for (auto &sh : shapes) {
+  for (int q = 0; q < nshape; q++) {
+    const int *sh = d->prec == DOUBLE ? shapes_dp[q] : shapes_mix[q];
     const int tpi = d->tpi ? d->tpi : sh[0];
     const int ip = d->ip ? d->ip : sh[1];
     const int ti = force_tile_i(tpi, ip);
@@ -559,9 +563,10 @@ int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double e
 
 int sapb_set_launch(sapb_dev *d, int tpi, int ip, int nslices) {
   if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
-  const bool ok_tpi = tpi == 0 || tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8 ||
-                      ((tpi == 16 || tpi == 32) && ip == 1);
-  if (!ok_tpi || (ip != 0 && ip != 1 && ip != 2) || nslices < 0 || (tpi && !ip))
+  const bool ok_tpi = tpi == 0 || ((tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8) && ip <= 2) ||
+                      ((tpi == 16 || tpi == 32) && ip == 1) ||
+                      ((tpi == 1 || tpi == 2) && ip == 4 && d->prec != DOUBLE);
+  if (!ok_tpi || (ip != 0 && ip != 1 && ip != 2 && ip != 4) || nslices < 0 || (tpi && !ip))
     return fail(d, SAPB_EINVAL, "unsupported launch shape tpi=%d ip=%d slices=%d", tpi, ip, nslices);
   d->tpi = tpi;
   d->ip = ip;

@@ -146,27 +146,33 @@ __global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti,
 // ========================================================================
 // Force kernel.
 //
-// Block = 128 threads laid out as TPI rows x TIT = 128/TPI columns; each
-// thread owns IP i-particles (columns tx, tx+TIT, ...), so a block covers an
-// i-tile of TI = TIT*IP particles.  blockIdx.y selects a j-slice of
-// `slice_tiles` tiles of TJ = 128 records.  Thread 0 streams the slice's
-// tiles into a 3-stage shared-memory ring with cp.async.bulk and mbarrier
-// completion; row `ty` of the block consumes records ty, ty+TPI, ... of
-// each tile.
+// Block = 4 warps, laid out as TPI rows x TIT = 128/TPI columns; each thread
+// owns IP i-particles (columns tx, tx+TIT, ...), so a block covers an i-tile
+// of TI = TIT*IP particles.  blockIdx.y selects a j-slice of `slice_tiles`
+// tiles of TJ = 128 records.  Lane 0 of warp 0 streams the slice's tiles
+// into a 3-stage shared-memory ring with cp.async.bulk (TMA engine): `full`
+// mbarriers signal arrival (complete_tx), `empty` mbarriers collect one
+// arrival per warp; there is no block-wide barrier per tile, so warps drift
+// up to two tiles apart instead of waiting for the slowest one.
+// Row `ty` consumes records ty, ty+TPI, ... of each tile.
 //
 // Mixed precision (DOUBLESINGLE): dr = (xj_hi - xi_hi) + (xj_lo - xi_lo)
 // in FP32 (double-single difference, kernels.cu:169-177), FP32 body with
-// rsqrt on the MUFU pipe, FP32 sums per tile folded into FP64 totals after
-// every tile.  FP64 (DOUBLE): every step in double, rsqrt(double).
+// rsqrt on the MUFU pipe (two i per thread as packed FP32x2), FP32 sums per
+// tile folded into FP64 totals (shared memory) after every tile.
+// FP64 (DOUBLE): every step in double, rsqrt(double).
 //
 // The self pair (id_i == id_j, kernels.cu:565) is removed by replacing dx
 // with a huge value, which makes ds2 ~ 1e36 (1e300 in FP64): its force
 // underflows to zero and it can be neither nearest neighbour nor listed.
 //
-// Nearest neighbour and neighbour list are found per tile: the pair loop
-// only keeps the tile's minimum ds2; when that minimum is below the current
-// best or below h2, the (rare) rescan recomputes ds2 bit-identically for the
-// tile and emits list entries / the best (ds2, id) key.
+// Nearest neighbour and neighbour list cost one FMNMX per pair: the pair
+// loop only keeps the tile's minimum ds2.  Neighbour list: when that minimum
+// is below h2, the warp rescans the tile cooperatively (lanes split the j)
+// and appends the hits.  Nearest neighbour: each thread remembers the tile
+// where its smallest ds2 first appeared and rescans only that tile, from L2,
+// after the loop.  Rescans recompute ds2 bit-identically (same rounded
+// operations).
 // ========================================================================
 constexpr int kBT = 128;
 constexpr int kTJ = 128;
@@ -182,10 +188,20 @@ struct FCfg {
   static constexpr int TILE_BYTES = kTJ * REC;
   static constexpr int RED_BYTES = TPI > 1 ? kBT * IP * kResStride * 8 : 0;
   static constexpr int BODY = kNS * TILE_BYTES > RED_BYTES ? kNS * TILE_BYTES : RED_BYTES;
-  static constexpr int SMEM = 128 + BODY;
+  // mixed precision keeps its FP64 running totals in shared memory (10 per
+  // i, [field][thread] so a warp's accesses are consecutive), which frees
+  // 40 registers per thread and lets 4 blocks share an SM
+  static constexpr int TOT_BYTES = PREC == DOUBLE ? 0 : IP * 10 * kBT * 8;
+  static constexpr int SMEM = 128 + BODY + TOT_BYTES;
+  static constexpr int MIN_BLOCKS = PREC == DOUBLE ? 1 : (IP >= 4 ? 2 : 4);
 };
 
 // ---------------- mixed precision pair ----------------
+// dr = (xj_hi - xi_hi) + (xj_lo - xi_lo) in FP32 (the double-single
+// difference of kernels.cu:169-177), everything after it in FP32 with rsqrt
+// on the MUFU pipe.  (A variant taking the difference in FP64 and rounding
+// once moved 9 FMA-pipe operations per pair to the FP64 and XU pipes but was
+// not faster: 3 FP64->FP32 conversions cost 24 XU cycles per warp and pair.)
 struct IMix {
   float xh, yh, zh, xl, yl, zl, vx, vy, vz, ax, ay, az, h2;
   int id;
@@ -252,6 +268,90 @@ __device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const 
   }
 }
 
+// ---------------- mixed precision, two i per thread, packed FP32x2 -------
+// The two i-particles of a thread travel in the .x/.y halves of float2
+// registers and every FP32 step is one sm_100 packed instruction
+// (__fadd2_rn / __fmul2_rn / __ffma2_rn) for both; j operands are
+// broadcast.  Per half the rounding is exactly that of the scalar path, so
+// ds2 here is bit-identical to pair_dr_mix (used by the rescans).
+struct IMix2 {
+  float2 nxh, nyh, nzh, nxl, nyl, nzl;  // negated hi / lo position parts
+  float2 nvx, nvy, nvz, nax, nay, naz;  // negated velocity, acceleration
+  int ida, idb;
+};
+struct AccMix2 {
+  float2 ax, ay, az, pot, jx, jy, jz, sx, sy, sz;  // pot accumulates +m/r
+};
+
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 neg2(float a, float b) { return make_float2(-a, -b); }
+
+__device__ __forceinline__ IMix2 pack_i2(const IMix &a, const IMix &b) {
+  IMix2 I;
+  I.nxh = neg2(a.xh, b.xh); I.nyh = neg2(a.yh, b.yh); I.nzh = neg2(a.zh, b.zh);
+  I.nxl = neg2(a.xl, b.xl); I.nyl = neg2(a.yl, b.yl); I.nzl = neg2(a.zl, b.zl);
+  I.nvx = neg2(a.vx, b.vx); I.nvy = neg2(a.vy, b.vy); I.nvz = neg2(a.vz, b.vz);
+  I.nax = neg2(a.ax, b.ax); I.nay = neg2(a.ay, b.ay); I.naz = neg2(a.az, b.az);
+  I.ida = a.id;
+  I.idb = b.id;
+  return I;
+}
+
+template <int ORDER>
+__device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, const float4 &r1,
+                                          const float4 &r2, const float4 &r3, float2 eps2,
+                                          AccMix2 &A, float2 &tmin) {
+  // x - y == x + (-y) exactly, so these equal ds_sub of the scalar path
+  float2 dx = __fadd2_rn(__fadd2_rn(bc2(r0.x), I.nxh), __fadd2_rn(bc2(r1.x), I.nxl));
+  const float2 dy = __fadd2_rn(__fadd2_rn(bc2(r0.y), I.nyh), __fadd2_rn(bc2(r1.y), I.nyl));
+  const float2 dz = __fadd2_rn(__fadd2_rn(bc2(r0.z), I.nzh), __fadd2_rn(bc2(r1.z), I.nzl));
+  const int idj = __float_as_int(r1.w);
+  dx.x = (idj == I.ida) ? 1.0e18f : dx.x;
+  dx.y = (idj == I.idb) ? 1.0e18f : dx.y;
+  const float2 ds2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+  tmin.x = fminf(tmin.x, ds2.x);
+  tmin.y = fminf(tmin.y, ds2.y);
+  const float2 r2v = __fadd2_rn(ds2, eps2);
+  const float2 inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
+  const float2 inv2 = __fmul2_rn(inv, inv);
+  const float2 minv = __fmul2_rn(bc2(r0.w), inv);
+  const float2 minv3 = __fmul2_rn(minv, inv2);
+  A.ax = __ffma2_rn(minv3, dx, A.ax);
+  A.ay = __ffma2_rn(minv3, dy, A.ay);
+  A.az = __ffma2_rn(minv3, dz, A.az);
+  A.pot = __fadd2_rn(A.pot, minv);
+  const float2 dvx = __fadd2_rn(bc2(r2.x), I.nvx);
+  const float2 dvy = __fadd2_rn(bc2(r2.y), I.nvy);
+  const float2 dvz = __fadd2_rn(bc2(r2.z), I.nvz);
+  const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
+  const float2 m3i2 = __fmul2_rn(bc2(-3.0f), inv2);
+  if (ORDER == FOURTH) {
+    const float2 c = __fmul2_rn(__fmul2_rn(m3i2, minv3), rv);
+    A.jx = __ffma2_rn(c, dx, __ffma2_rn(minv3, dvx, A.jx));
+    A.jy = __ffma2_rn(c, dy, __ffma2_rn(minv3, dvy, A.jy));
+    A.jz = __ffma2_rn(c, dz, __ffma2_rn(minv3, dvz, A.jz));
+  } else {
+    const float2 dax = __fadd2_rn(bc2(r3.x), I.nax);
+    const float2 day = __fadd2_rn(bc2(r3.y), I.nay);
+    const float2 daz = __fadd2_rn(bc2(r3.z), I.naz);
+    const float2 s = __ffma2_rn(dz, daz, __ffma2_rn(dy, day, __ffma2_rn(dx, dax,
+                     __ffma2_rn(dvz, dvz, __ffma2_rn(dvy, dvy, __fmul2_rn(dvx, dvx))))));
+    const float2 a3 = __fmul2_rn(m3i2, rv);
+    const float2 b3 = __ffma2_rn(a3, __fmul2_rn(a3, bc2(-1.0f / 3.0f)), __fmul2_rn(s, m3i2));
+    const float2 c6 = __fmul2_rn(__fadd2_rn(a3, a3), minv3);
+    const float2 tx = __ffma2_rn(a3, dx, dvx), ty = __ffma2_rn(a3, dy, dvy),
+                 tz = __ffma2_rn(a3, dz, dvz);
+    A.jx = __ffma2_rn(minv3, tx, A.jx);
+    A.jy = __ffma2_rn(minv3, ty, A.jy);
+    A.jz = __ffma2_rn(minv3, tz, A.jz);
+    const float2 ux = __ffma2_rn(b3, dx, dax), uy = __ffma2_rn(b3, dy, day),
+                 uz = __ffma2_rn(b3, dz, daz);
+    A.sx = __ffma2_rn(c6, tx, __ffma2_rn(minv3, ux, A.sx));
+    A.sy = __ffma2_rn(c6, ty, __ffma2_rn(minv3, uy, A.sy));
+    A.sz = __ffma2_rn(c6, tz, __ffma2_rn(minv3, uz, A.sz));
+  }
+}
+
 // ---------------- FP64 pair ----------------
 struct IDp {
   double x, y, z, vx, vy, vz, ax, ay, az, h2;
@@ -312,37 +412,124 @@ __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const d
   }
 }
 
-// Per-i running state kept across tiles.
-struct NNState {
-  unsigned long long key;  // best (ds2, id)
-  float best;              // ds2 part of key (float), -1 for padding i
-};
-
 __device__ __forceinline__ void list_push(int *cnt, int *list, int gi, int idj) {
   const int pos = atomicAdd(cnt + gi, 1);
   if (pos < kNgbPB) list[(size_t)gi * kNgbPB + pos] = idj;
 }
 
+// Warp-cooperative neighbour-list rescan of one shared-memory tile: for every
+// lane whose i saw a pair below h2 in this tile, the whole warp re-evaluates
+// that i against the tile's j (lane-strided) and appends the hits.
+template <int PREC, int RS, int TPI>
+__device__ __forceinline__ void list_rescan_mix(const IMix &I, bool want, int gi, int row,
+                                                const float4 *rec, int cnt, int lane,
+                                                int *ngb_count, int *ngb_list) {
+  unsigned m = __ballot_sync(0xffffffffu, want);
+  while (m) {
+    const int src = __ffs(m) - 1;
+    m &= m - 1;
+    IMix S;
+    S.xh = __shfl_sync(0xffffffffu, I.xh, src);
+    S.yh = __shfl_sync(0xffffffffu, I.yh, src);
+    S.zh = __shfl_sync(0xffffffffu, I.zh, src);
+    S.xl = __shfl_sync(0xffffffffu, I.xl, src);
+    S.yl = __shfl_sync(0xffffffffu, I.yl, src);
+    S.zl = __shfl_sync(0xffffffffu, I.zl, src);
+    S.h2 = __shfl_sync(0xffffffffu, I.h2, src);
+    S.id = __shfl_sync(0xffffffffu, I.id, src);
+    const int sgi = __shfl_sync(0xffffffffu, gi, src);
+    const int srow = __shfl_sync(0xffffffffu, row, src);
+    for (int k = srow + lane * TPI; k < cnt; k += 32 * TPI) {
+      float dx, dy, dz;
+      const float4 r0 = rec[k * RS + 0];
+      const float4 r1 = rec[k * RS + 1];
+      const float ds2 = pair_dr_mix(S, r0, r1, dx, dy, dz);
+      if (ds2 < S.h2) list_push(ngb_count, ngb_list, sgi, __float_as_int(r1.w));
+    }
+  }
+}
+
+template <int PREC, int RS, int TPI>
+__device__ __forceinline__ void list_rescan_dp(const IDp &I, bool want, int gi, int row,
+                                               const double4 *rec, int cnt, int lane,
+                                               int *ngb_count, int *ngb_list) {
+  unsigned m = __ballot_sync(0xffffffffu, want);
+  while (m) {
+    const int src = __ffs(m) - 1;
+    m &= m - 1;
+    IDp S;
+    S.x = __shfl_sync(0xffffffffu, I.x, src);
+    S.y = __shfl_sync(0xffffffffu, I.y, src);
+    S.z = __shfl_sync(0xffffffffu, I.z, src);
+    S.h2 = __shfl_sync(0xffffffffu, I.h2, src);
+    S.id = __shfl_sync(0xffffffffu, I.id, src);
+    const int sgi = __shfl_sync(0xffffffffu, gi, src);
+    const int srow = __shfl_sync(0xffffffffu, row, src);
+    for (int k = srow + lane * TPI; k < cnt; k += 32 * TPI) {
+      double dx, dy, dz;
+      const double4 r0 = rec[k * RS + 0];
+      const double4 r1 = rec[k * RS + 1];
+      const double ds2 = pair_dr_dp(S, r0, r1, dx, dy, dz);
+      if (ds2 < S.h2) list_push(ngb_count, ngb_list, sgi, __double2loint(r1.w));
+    }
+  }
+}
+
 template <int ORDER, int PREC, int TPI, int IP>
-__global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
+__global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
+    force_kernel(ForceArgs A) {
   using C = FCfg<ORDER, PREC, TPI, IP>;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *empty = full + kNS;
   unsigned char *tiles = smem + 128;
 
   const int tid = threadIdx.x;
-  const int tx = tid % C::TIT;
-  const int ty = tid / C::TIT;
+  const int lane = tid & 31;
   const int itile = blockIdx.x;
   const int slice = blockIdx.y;
-  const int istr = i_stride(ORDER);
 
-  // ---- i-particles of this thread ----
+  // ---- j range of this slice ----
+  const int ntiles_all = (A.nj + kTJ - 1) / kTJ;
+  const int t0 = slice * A.slice_tiles;
+  const int t1 = min(t0 + A.slice_tiles, ntiles_all);
+  const int nt = max(t1 - t0, 0);
+  const unsigned char *pred = reinterpret_cast<const unsigned char *>(A.pred);
+
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < kNS; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kBT / 32);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  // ---- producer: lane 0 of warp 0 fills the ring ----
+  auto issue = [&](int it) {
+    const int st = it % kNS;
+    const int tile = t0 + it;
+    const int cnt = min(kTJ, A.nj - tile * kTJ);
+    const uint32_t bytes = (uint32_t)(cnt * C::REC);
+    fence_proxy_async();
+    mbar_expect_tx(&full[st], bytes);
+    bulk_g2s(tiles + st * C::TILE_BYTES, pred + (size_t)tile * kTJ * C::REC, bytes, &full[st]);
+  };
+  const bool producer = (tid == 0);
+  if (producer)
+    for (int it = 0; it < kNS && it < nt; it++) issue(it);
+
+  // ---- consumers: 128 threads = TPI rows x TIT columns, IP i each ----
+  const int tx = tid % C::TIT;
+  const int ty = tid / C::TIT;
+  const int istr = i_stride(ORDER);
   int gi[IP];
   bool valid[IP];
   IMix Im[IP];
   IDp Id[IP];
-  NNState nn[IP];
+  float best[IP];     // smallest ds2 seen (float), -1 for padding i
+  int best_tile[IP];  // tile (within the slice) where it was first seen
 #pragma unroll
   for (int p = 0; p < IP; p++) {
     gi[p] = itile * C::TI + p * C::TIT + tx;
@@ -365,49 +552,37 @@ __global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
                    (float)(z - (double)hz), (float)vx, (float)vy, (float)vz, (float)ax,
                    (float)ay, (float)az, valid[p] ? (float)h2 : -1.0f, id};
     }
-    nn[p].key = nn_key(kNoNgbDs2, -1);
-    nn[p].best = valid[p] ? kNoNgbDs2 : -1.0f;
-  }
-
-  // ---- j range of this slice ----
-  const int ntiles_all = (A.nj + kTJ - 1) / kTJ;
-  const int t0 = slice * A.slice_tiles;
-  const int t1 = min(t0 + A.slice_tiles, ntiles_all);
-  const int nt = max(t1 - t0, 0);
-  const unsigned char *pred = reinterpret_cast<const unsigned char *>(A.pred);
-
-  if (tid == 0) {
-#pragma unroll
-    for (int s = 0; s < kNS; s++) mbar_init(&bars[s], 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  auto issue = [&](int it) {
-    const int tile = t0 + it;
-    const int cnt = min(kTJ, A.nj - tile * kTJ);
-    const uint32_t bytes = (uint32_t)(cnt * C::REC);
-    uint64_t *bar = &bars[it % kNS];
-    mbar_expect_tx(bar, bytes);
-    bulk_g2s(tiles + (it % kNS) * C::TILE_BYTES, pred + (size_t)tile * kTJ * C::REC, bytes, bar);
-  };
-  if (tid == 0) {
-    for (int s = 0; s < kNS && s < nt; s++) issue(s);
+    best[p] = valid[p] ? kNoNgbDs2 : -1.0f;
+    best_tile[p] = -1;
   }
 
   AccDp D[IP];
 #pragma unroll
   for (int p = 0; p < IP; p++) D[p] = AccDp{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double *tot = reinterpret_cast<double *>(tiles + C::BODY);  // mixed: [p][field][tid]
+  if (PREC != DOUBLE) {
+#pragma unroll
+    for (int q = 0; q < IP * 10; q++) tot[q * kBT + tid] = 0.0;
+  }
   const float eps2f = (float)A.eps2;
+  const float2 eps2v = make_float2(eps2f, eps2f);
+  constexpr int NPAIR = IP / 2;  // packed i pairs per thread (mixed precision)
+  IMix2 I2[NPAIR > 0 ? NPAIR : 1];
+  if (PREC != DOUBLE) {
+#pragma unroll
+    for (int q = 0; q < NPAIR; q++) I2[q] = pack_i2(Im[2 * q], Im[(2 * q + 1) % IP]);
+  }
   bool broken = false;
 
   for (int it = 0; it < nt; it++) {
-    if (!broken && !mbar_wait_bounded(&bars[it % kNS], (uint32_t)((it / kNS) & 1))) {
+    const int s = it % kNS;
+    if (!broken && !mbar_wait_bounded(&full[s], (uint32_t)((it / kNS) & 1))) {
       broken = true;
       atomicOr(A.status, kErrWaitTimeout);
     }
     const int tile = t0 + it;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
-    const unsigned char *buf = tiles + (it % kNS) * C::TILE_BYTES;
+    const unsigned char *buf = tiles + s * C::TILE_BYTES;
 
     if (PREC == DOUBLE) {
       const double4 *rec = reinterpret_cast<const double4 *>(buf);
@@ -424,23 +599,14 @@ __global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
       }
 #pragma unroll
       for (int p = 0; p < IP; p++) {
-        const bool want_list = A.do_list && tmin[p] < Id[p].h2;
-        const bool want_nn = (float)tmin[p] <= nn[p].best;
-        if (want_list || want_nn) {
-          unsigned long long key = nn[p].key;
-          for (int k = ty; k < cnt; k += TPI) {
-            double dx, dy, dz;
-            const double4 r0 = rec[k * C::RS + 0];
-            const double4 r1 = rec[k * C::RS + 1];
-            const double ds2 = pair_dr_dp(Id[p], r0, r1, dx, dy, dz);
-            const int idj = __double2loint(r1.w);
-            if (want_list && ds2 < Id[p].h2) list_push(A.ngb_count, A.ngb_list, gi[p], idj);
-            const float f2 = (float)ds2;
-            if (want_nn && f2 < kNoNgbDs2) key = min(key, nn_key(f2, idj));
-          }
-          nn[p].key = key;
-          nn[p].best = __uint_as_float((unsigned int)(key >> 32));
+        const float tf = (float)tmin[p];
+        if (tf < best[p]) {
+          best[p] = tf;
+          best_tile[p] = it;
         }
+        if (A.do_list)
+          list_rescan_dp<PREC, C::RS, TPI>(Id[p], tmin[p] < Id[p].h2, gi[p], ty, rec, cnt, lane,
+                                           A.ngb_count, A.ngb_list);
       }
     } else {
       const float4 *rec = reinterpret_cast<const float4 *>(buf);
@@ -451,63 +617,129 @@ __global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
         P[p] = AccMix{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         tmin[p] = FLT_MAX;
       }
-#pragma unroll 2
-      for (int k = ty; k < cnt; k += TPI) {
-        const float4 r0 = rec[k * C::RS + 0];
-        const float4 r1 = rec[k * C::RS + 1];
-        const float4 r2 = rec[k * C::RS + 2];
-        const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+      if constexpr (IP % 2 == 0) {
+        AccMix2 Q[NPAIR];
+        float2 tm[NPAIR];
+        const float2 z2 = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int p = 0; p < IP; p++) pair_mix<ORDER>(Im[p], r0, r1, r2, r3, eps2f, P[p], tmin[p]);
+        for (int q = 0; q < NPAIR; q++) {
+          Q[q] = AccMix2{z2, z2, z2, z2, z2, z2, z2, z2, z2, z2};
+          tm[q] = make_float2(FLT_MAX, FLT_MAX);
+        }
+#pragma unroll 2
+        for (int k = ty; k < cnt; k += TPI) {
+          const float4 r0 = rec[k * C::RS + 0];
+          const float4 r1 = rec[k * C::RS + 1];
+          const float4 r2 = rec[k * C::RS + 2];
+          const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+#pragma unroll
+          for (int q = 0; q < NPAIR; q++) pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < NPAIR; q++) {
+          P[2 * q] = AccMix{Q[q].ax.x, Q[q].ay.x, Q[q].az.x, -Q[q].pot.x, Q[q].jx.x, Q[q].jy.x,
+                            Q[q].jz.x, Q[q].sx.x, Q[q].sy.x, Q[q].sz.x};
+          P[2 * q + 1] = AccMix{Q[q].ax.y, Q[q].ay.y, Q[q].az.y, -Q[q].pot.y, Q[q].jx.y,
+                                Q[q].jy.y, Q[q].jz.y, Q[q].sx.y, Q[q].sy.y, Q[q].sz.y};
+          tmin[2 * q] = tm[q].x;
+          tmin[2 * q + 1] = tm[q].y;
+        }
+      } else {
+#pragma unroll 2
+        for (int k = ty; k < cnt; k += TPI) {
+          const float4 r0 = rec[k * C::RS + 0];
+          const float4 r1 = rec[k * C::RS + 1];
+          const float4 r2 = rec[k * C::RS + 2];
+          const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+#pragma unroll
+          for (int p = 0; p < IP; p++)
+            pair_mix<ORDER>(Im[p], r0, r1, r2, r3, eps2f, P[p], tmin[p]);
+        }
       }
 #pragma unroll
       for (int p = 0; p < IP; p++) {
-        D[p].ax += (double)P[p].ax;
-        D[p].ay += (double)P[p].ay;
-        D[p].az += (double)P[p].az;
-        D[p].pot += (double)P[p].pot;
-        D[p].jx += (double)P[p].jx;
-        D[p].jy += (double)P[p].jy;
-        D[p].jz += (double)P[p].jz;
+        double *t = tot + (size_t)p * 10 * kBT + tid;
+        t[0 * kBT] += (double)P[p].ax;
+        t[1 * kBT] += (double)P[p].ay;
+        t[2 * kBT] += (double)P[p].az;
+        t[3 * kBT] += (double)P[p].pot;
+        t[4 * kBT] += (double)P[p].jx;
+        t[5 * kBT] += (double)P[p].jy;
+        t[6 * kBT] += (double)P[p].jz;
         if (ORDER >= SIXTH) {
-          D[p].sx += (double)P[p].sx;
-          D[p].sy += (double)P[p].sy;
-          D[p].sz += (double)P[p].sz;
+          t[7 * kBT] += (double)P[p].sx;
+          t[8 * kBT] += (double)P[p].sy;
+          t[9 * kBT] += (double)P[p].sz;
         }
-        const bool want_list = A.do_list && tmin[p] < Im[p].h2;
-        const bool want_nn = tmin[p] <= nn[p].best;
-        if (want_list || want_nn) {
-          unsigned long long key = nn[p].key;
-          for (int k = ty; k < cnt; k += TPI) {
-            float dx, dy, dz;
-            const float4 r0 = rec[k * C::RS + 0];
-            const float4 r1 = rec[k * C::RS + 1];
-            const float ds2 = pair_dr_mix(Im[p], r0, r1, dx, dy, dz);
-            const int idj = __float_as_int(r1.w);
-            if (want_list && ds2 < Im[p].h2) list_push(A.ngb_count, A.ngb_list, gi[p], idj);
-            if (want_nn && ds2 < kNoNgbDs2) key = min(key, nn_key(ds2, idj));
-          }
-          nn[p].key = key;
-          nn[p].best = __uint_as_float((unsigned int)(key >> 32));
+        if (tmin[p] < best[p]) {
+          best[p] = tmin[p];
+          best_tile[p] = it;
         }
+        if (A.do_list)
+          list_rescan_mix<PREC, C::RS, TPI>(Im[p], tmin[p] < Im[p].h2, gi[p], ty, rec, cnt, lane,
+                                            A.ngb_count, A.ngb_list);
       }
     }
-    __syncthreads();  // every thread is done with this stage's buffer
-    if (tid == 0 && !broken && it + kNS < nt) {
-      fence_proxy_async();
-      issue(it + kNS);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
+    // Refill the stage once all four warps released it; only warp 0 waits
+    // here, the others may already be up to kNS-1 tiles ahead.
+    if (producer && !broken && it + kNS < nt) {
+      if (mbar_wait_bounded(&empty[s], (uint32_t)((it / kNS) & 1))) {
+        issue(it + kNS);
+      } else {
+        broken = true;
+        atomicOr(A.status, kErrWaitTimeout);
+      }
     }
   }
   if (broken && tid == 0) {
-    // Let copies still in flight land before the block's shared memory is
-    // released (bounded; the error is already recorded).
+    // let copies still in flight land before shared memory is released
     for (int it = max(nt - kNS, 0); it < nt; it++)
-      mbar_wait_bounded(&bars[it % kNS], (uint32_t)((it / kNS) & 1));
+      mbar_wait_bounded(&full[it % kNS], (uint32_t)((it / kNS) & 1));
+  }
+
+  if (PREC != DOUBLE) {
+#pragma unroll
+    for (int p = 0; p < IP; p++) {
+      const double *t = tot + (size_t)p * 10 * kBT + tid;
+      D[p] = AccDp{t[0], t[kBT], t[2 * kBT], t[3 * kBT], t[4 * kBT], t[5 * kBT], t[6 * kBT],
+                   t[7 * kBT], t[8 * kBT], t[9 * kBT]};
+    }
+  }
+
+  // ---- nearest neighbour: one rescan of the best tile (from L2) ----
+  unsigned long long key[IP];
+#pragma unroll
+  for (int p = 0; p < IP; p++) {
+    key[p] = nn_key(kNoNgbDs2, -1);
+    if (best_tile[p] < 0) continue;
+    const int tile = t0 + best_tile[p];
+    const int cnt = min(kTJ, A.nj - tile * kTJ);
+    if (PREC == DOUBLE) {
+      const double4 *rec = reinterpret_cast<const double4 *>(pred + (size_t)tile * kTJ * C::REC);
+      for (int k = ty; k < cnt; k += TPI) {
+        double dx, dy, dz;
+        const double4 r0 = rec[k * C::RS + 0];
+        const double4 r1 = rec[k * C::RS + 1];
+        const float f2 = (float)pair_dr_dp(Id[p], r0, r1, dx, dy, dz);
+        if (f2 < kNoNgbDs2) key[p] = min(key[p], nn_key(f2, __double2loint(r1.w)));
+      }
+    } else {
+      const float4 *rec = reinterpret_cast<const float4 *>(pred + (size_t)tile * kTJ * C::REC);
+      for (int k = ty; k < cnt; k += TPI) {
+        float dx, dy, dz;
+        const float4 r0 = __ldg(rec + k * C::RS + 0);
+        const float4 r1 = __ldg(rec + k * C::RS + 1);
+        const float ds2 = pair_dr_mix(Im[p], r0, r1, dx, dy, dz);
+        if (ds2 < kNoNgbDs2) key[p] = min(key[p], nn_key(ds2, __float_as_int(r1.w)));
+      }
+    }
   }
 
   // ---- combine rows (threads-per-i > 1), fixed order ----
   if (TPI > 1) {
-    __syncthreads();
+    named_barrier(1, kBT);  // all consumer warps are past their last tile
     double *red = reinterpret_cast<double *>(tiles);
 #pragma unroll
     for (int p = 0; p < IP; p++) {
@@ -515,9 +747,9 @@ __global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
       o[0] = D[p].ax; o[1] = D[p].ay; o[2] = D[p].az; o[3] = D[p].pot;
       o[4] = D[p].jx; o[5] = D[p].jy; o[6] = D[p].jz;
       o[7] = D[p].sx; o[8] = D[p].sy; o[9] = D[p].sz;
-      o[10] = __longlong_as_double((long long)nn[p].key);
+      o[10] = __longlong_as_double((long long)key[p]);
     }
-    __syncthreads();
+    named_barrier(1, kBT);
     if (ty != 0) return;
 #pragma unroll
     for (int p = 0; p < IP; p++) {
@@ -526,7 +758,7 @@ __global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
         D[p].ax += o[0]; D[p].ay += o[1]; D[p].az += o[2]; D[p].pot += o[3];
         D[p].jx += o[4]; D[p].jy += o[5]; D[p].jz += o[6];
         D[p].sx += o[7]; D[p].sy += o[8]; D[p].sz += o[9];
-        nn[p].key = min(nn[p].key, (unsigned long long)__double_as_longlong(o[10]));
+        key[p] = min(key[p], (unsigned long long)__double_as_longlong(o[10]));
       }
     }
   }
@@ -541,11 +773,11 @@ __global__ void __launch_bounds__(kBT) force_kernel(ForceArgs A) {
     o[4] = D[p].jx; o[5] = D[p].jy; o[6] = D[p].jz;
     o[7] = D[p].sx; o[8] = D[p].sy; o[9] = D[p].sz;
     if (A.write_partials) {
-      o[10] = __longlong_as_double((long long)nn[p].key);
+      o[10] = __longlong_as_double((long long)key[p]);
       o[11] = 0.0;
     } else {
-      o[10] = (double)__uint_as_float((unsigned int)(nn[p].key >> 32));
-      o[11] = (double)(int)(unsigned int)(nn[p].key & 0xffffffffu);
+      o[10] = (double)__uint_as_float((unsigned int)(key[p] >> 32));
+      o[11] = (double)(int)(unsigned int)(key[p] & 0xffffffffu);
     }
   }
 }
@@ -635,7 +867,13 @@ static cudaError_t launch_force_t(const ForceArgs &A, cudaStream_t st) {
 
 template <int ORDER, int PREC>
 static cudaError_t launch_force_o(const ForceArgs &A, int tpi, int ip, cudaStream_t st) {
-  if (ip == 2) {
+  if (ip == 4 && PREC != DOUBLE) {
+    switch (tpi) {
+      case 1: return launch_force_t<ORDER, PREC, 1, 4>(A, st);
+      case 2: return launch_force_t<ORDER, PREC, 2, 4>(A, st);
+      default: break;
+    }
+  } else if (ip == 2) {
     switch (tpi) {
       case 1: return launch_force_t<ORDER, PREC, 1, 2>(A, st);
       case 2: return launch_force_t<ORDER, PREC, 2, 2>(A, st);

@@ -47,16 +47,22 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+// One suspending probe of phase `parity`: the hardware may park the thread
+// for a bounded time inside try_wait, so waiting warps do not burn issue
+// slots of the warps that compute.
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
   return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ uint64_t global_timer_ns() {
   uint64_t t;
@@ -65,17 +71,21 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 }
 // Waits for phase `parity` of `bar`, giving up after ~2 s of wall time.
 // Returns false on timeout; the caller records the error and carries on
-// (every thread still reaches every block barrier, so nothing hangs).
+// without waiting again, so no thread can hang.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  if (mbar_test(bar, parity)) return true;
+  if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (;;) {
 #pragma unroll 1
-    for (int k = 0; k < 256; k++)
-      if (mbar_test(bar, parity)) return true;
+    for (int k = 0; k < 64; k++)
+      if (mbar_try(bar, parity)) return true;
     if (global_timer_ns() - t0 > 2000000000ull) return false;
-    __nanosleep(100);
   }
+}
+// Barrier among the `nthreads` consumer threads only (id 1; id 0 is
+// __syncthreads).
+__device__ __forceinline__ void named_barrier(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 __device__ __forceinline__ float rsqrt_mufu(float x) {

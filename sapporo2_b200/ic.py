@@ -149,7 +149,9 @@ def make_config(name: str, n: int | None = None, seed: int | None = None) -> dic
         all active, lists off.
     C2  Plummer equal mass, 6th order, block steps dt = 2^-k (k in 3..12),
         h2 for ~32 neighbours, lists on.
-    C3  Plummer + Salpeter masses + 10 % circular binaries, 6th order.
+    C3  Plummer + Salpeter masses + 10 % circular binaries, 6th order,
+        t0 = t_i - U{0..7} 2^-10, all active.
+    C5  Plummer equal mass + 10 % circular binaries, 6th order, lists on.
     """
     defaults = {"C1": (16384, 1), "C2": (131072, 2), "C3": (1 << 20, 3), "C5": (262144, 5)}
     n0, s0 = defaults[name]
@@ -174,7 +176,7 @@ def make_config(name: str, n: int | None = None, seed: int | None = None) -> dic
         x, v, m = plummer(n, seed, masses=m)
         x, v, m, pairs = add_binaries(x, v, m, 0.10, seed + 11)
         cfg.update(order=2, x=x, v=v, m=m, pairs=pairs, ti=1.0)
-        cfg["t0"] = np.full(n, 1.0)
+        cfg["t0"] = cfg["ti"] - rng.integers(0, 8, n) * 2.0 ** -10
         cfg["h2"] = plummer_h2(x, m, 32.0)
         cfg["lists"] = name == "C5"
     cfg["id"] = np.arange(n, dtype=np.int32)
@@ -195,3 +197,19 @@ def fill_derivatives(cfg: dict, force_fn) -> dict:
         cfg["s"] = snp
         cfg["c"] = crackle_from(x, acc, jrk)
     return cfg
+
+
+def predict_fp64(order: int, ti: float, t0, x, v, a, j, s=None, c=None):
+    """FP64 Taylor prediction to ti in the Horner form of the device
+    predictor (used to build the i-particle inputs of the workloads)."""
+    dt = (ti - np.asarray(t0))[:, None]
+    dt2, dt3 = dt * (1.0 / 2.0), dt * (1.0 / 3.0)
+    if order >= 2:
+        dt4, dt5 = dt * (1.0 / 4.0), dt * (1.0 / 5.0)
+        px = x + dt * (v + dt2 * (a + dt3 * (j + dt4 * (s + dt5 * c))))
+        pv = v + dt * (a + dt2 * (j + dt3 * (s + dt4 * c)))
+        pa = a + dt * (j + dt2 * (s + dt3 * c))
+        return px, pv, pa
+    px = x + dt * (v + dt2 * (a + dt3 * j))
+    pv = v + dt * (a + dt2 * j)
+    return px, pv, None
