@@ -120,6 +120,31 @@ int sapb_ngb_fetch(sapb_dev *d, int *counts, int *lists, int ni);
 int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
                       double *res_dev, int *ngb_count_dev, int *ngb_list_dev);
 
+/* Force call that allocates nothing: no cudaMalloc, cudaFree or other
+ * allocating routine, on any call.  It is for callers that cannot allocate
+ * device memory while they integrate -- codes that hand the whole GPU to
+ * their own pool allocator, or that must not take the device-wide
+ * synchronisation cudaFree implies in the middle of a time step -- whereas
+ * sapb_force_device grows its partial-sum buffer with cudaMalloc/cudaFree
+ * when a larger active set arrives.  This build-specific entry point has no
+ * counterpart in the reference.
+ *
+ * Same arguments, layouts and results as sapb_force_device.  The j-split
+ * partial sums go to one fixed 32 MiB device array (SAPB_NOALLOC_SCRATCH_
+ * BYTES) that every GPU loading the library holds until exit; ni is limited
+ * to SAPB_NOALLOC_SCRATCH_BYTES / (8 * SAPB_RES_STRIDE) = 349525 per call
+ * (larger ni returns SAPB_EINVAL with a message), and the j-split is capped
+ * to fit.  The array's device address is resolved once per device by
+ * sapb_open (or by the first call on that device, which should then come
+ * before any stream capture).  All calls on a device share the array and it
+ * keeps the last call's contents (each call overwrites every record it
+ * reads, so nothing needs clearing); calls that overlap on the GPU --
+ * different streams or handles on one device -- race on it. */
+#define SAPB_NOALLOC_SCRATCH_BYTES (32u << 20)
+int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2,
+                              int flags, double *res_dev, int *ngb_count_dev,
+                              int *ngb_list_dev);
+
 /* FP64 state of j[first, first+n), 24 doubles per j:
  *   x[3] mass v[3] eps acc[3] jerk[3] px[3] pv[3] pa[3] id
  * where px/pv/pa are the FP64 prediction to ti (predict != 0) or the raw

@@ -28,6 +28,7 @@ GRAPE5, FOURTH, SIXTH = 0, 1, 2
 FLOAT, DOUBLESINGLE, DOUBLE = 0, 1, 2
 NGB_PB = 256
 NPIPES = 16384
+NOALLOC_SCRATCH_BYTES = 32 << 20  # fixed scratch of sapb_force_device_noalloc
 RES_STRIDE = 12
 F_PREDICT = 1
 F_NGB_LIST = 2
@@ -83,6 +84,9 @@ _SIGS = [
     ("sapb_ngb_fetch", C.c_int, [C.c_void_p, _ipo, _ipo, C.c_int]),
     ("sapb_force_device", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double,
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("sapb_force_device_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                            C.c_double, C.c_int, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]),
     ("sapb_read_j", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _dp]),
     ("sapb_set_launch", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     ("sapb_get_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 3),

@@ -255,6 +255,33 @@ static Plan make_plan(const sapb_dev *d, int ni, int nj) {
 }
 
 // ---------------------------------------------------------------------
+// Fixed scratch of sapb_force_device_noalloc.  Every GPU that loads this
+// library holds these 32 MiB until the process exits.  Host code must not
+// use the symbol itself (in host code it names a host-side stand-in, not
+// device memory): its device address is resolved once per device with
+// cudaGetSymbolAddress, with that device current, and passed to the kernels.
+// ---------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_scratch[SAPB_NOALLOC_SCRATCH_BYTES / 8];
+
+constexpr int kMaxDevices = 64;
+static double *g_noalloc_ptr[kMaxDevices];
+
+// Resolves the scratch address for the current device (once per device).
+static int noalloc_setup(sapb_dev *d) {
+  if (d->device < 0 || d->device >= kMaxDevices)
+    return fail(d, SAPB_EINVAL, "device ordinal %d beyond the no-allocation table", d->device);
+  if (g_noalloc_ptr[d->device]) return SAPB_OK;
+  CK(d, cudaSetDevice(d->device));
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr)
+    return fail(d, SAPB_ECUDA, "cudaGetSymbolAddress(no-allocation scratch): %s",
+                cudaGetErrorString(e));
+  g_noalloc_ptr[d->device] = static_cast<double *>(ptr);
+  return SAPB_OK;
+}
+
+// ---------------------------------------------------------------------
 extern "C" {
 
 const char *sapb_version(void) { return "sapporo-b200 0.1 (sm_100a)"; }
@@ -328,6 +355,8 @@ int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
     rc = grow_j(d, nj_reserve > 0 ? nj_reserve : 16384);
     if (rc) break;
     rc = ensure_i(d, d->n_pipes);
+    if (rc) break;
+    rc = noalloc_setup(d);
     if (rc) break;
     if (cudaStreamSynchronize(d->stream) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "sync"); break; }
   } while (0);
@@ -559,6 +588,56 @@ int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double e
   CK(d, cudaSetDevice(d->device));
   if (ni == 0) return SAPB_OK;
   return run_force(d, nj, ni, i_dev, eps2, flags, res_dev, ngb_count_dev, ngb_list_dev);
+}
+
+int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2,
+                              int flags, double *res_dev, int *ngb_count_dev,
+                              int *ngb_list_dev) {
+  if (!d || !i_dev || !res_dev || ni < 0) return fail(d, SAPB_EINVAL, "bad arguments");
+  if ((flags & SAPB_F_NGB_LIST) && (!ngb_count_dev || !ngb_list_dev))
+    return fail(d, SAPB_EINVAL, "neighbour lists requested without buffers");
+  const size_t cap_records = SAPB_NOALLOC_SCRATCH_BYTES / (sizeof(double) * kResStride);
+  if ((size_t)ni > cap_records)
+    return fail(d, SAPB_EINVAL,
+                "sapb_force_device_noalloc: ni = %d exceeds the fixed scratch (at most %zu "
+                "i-particles per call)", ni, cap_records);
+  if (nj <= 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "nj = %d (capacity %d)", nj, d->cap);
+  CK(d, cudaSetDevice(d->device));
+  if (ni == 0) return SAPB_OK;
+  int rc = noalloc_setup(d);  // normally already done by sapb_open
+  if (rc) return rc;
+  double *scratch = g_noalloc_ptr[d->device];
+  // Same plan as sapb_force_device, with the j-split capped so that the
+  // per-slice partial records fit the fixed scratch.
+  Plan P = make_plan(d, ni, nj);
+  const int tj = force_tile_j();
+  const int ntiles = (nj + tj - 1) / tj;
+  const int max_ns = (int)std::max<size_t>(1, cap_records / (size_t)ni);
+  if (P.ns > max_ns) {
+    P.slice_tiles = (ntiles + max_ns - 1) / max_ns;
+    P.ns = (ntiles + P.slice_tiles - 1) / P.slice_tiles;
+  }
+  const bool list = (flags & SAPB_F_NGB_LIST) != 0;
+  if (list) CK(d, cudaMemsetAsync(ngb_count_dev, 0, sizeof(int) * (size_t)ni, d->stream));
+  ForceArgs A{};
+  A.pred = d->pred;
+  A.nj = nj;
+  A.irec = i_dev;
+  A.ni = ni;
+  A.eps2 = eps2;
+  A.nslices = P.ns;
+  A.slice_tiles = P.slice_tiles;
+  A.i_tiles = P.i_tiles;
+  A.do_list = list ? 1 : 0;
+  A.ngb_count = ngb_count_dev;
+  A.ngb_list = ngb_list_dev;
+  A.status = d->status_d;
+  A.out = scratch;  // every (slice, valid i) record is written before it is read
+  A.write_partials = 1;
+  CK(d, launch_force(d->order, d->prec, A, P.tpi, P.ip, d->stream));
+  ReduceArgs R{scratch, P.ns, ni, res_dev, ngb_count_dev};
+  CK(d, launch_reduce(R, d->stream));
+  return SAPB_OK;
 }
 
 int sapb_set_launch(sapb_dev *d, int tpi, int ip, int nslices) {
