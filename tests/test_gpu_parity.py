@@ -34,10 +34,12 @@ def test_mixed_kernel_matches_oracle(gpu, order):
 
 @pytest.mark.parametrize("order,precision", [(1, 1), (2, 1), (2, 2)])
 @pytest.mark.parametrize("launch", [(1, 2, 0), (2, 2, 3), (4, 2, 0), (8, 2, 5), (16, 1, 2),
-                                    (32, 1, 0), (1, 1, 7)])
+                                    (32, 1, 0), (1, 1, 7), (1, 4, 0), (2, 4, 3)])
 def test_launch_shapes_agree(gpu, order, precision, launch):
     """Every (threads-per-i, i-per-thread, j-slices) shape gives the same
     physics; ragged i and j counts exercise the partial tiles."""
+    if launch[1] == 4 and precision == sp.DOUBLE:
+        pytest.skip("4 i per thread is a mixed-precision shape")
     case = T.build_case(order, 1000, seed=13, binaries=0.1)
     sel = np.arange(3, 900, 2)
     want = T.oracle_force(case, sel=sel)
