@@ -23,6 +23,7 @@ INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
 LIBDIR = PKG / "lib"
 LIBNAME = "libsapporo_b200.so"
+LIB6TH = "libsapporo6th_b200.so"  # 6th-order C interface (generic names, own library)
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
@@ -84,11 +85,20 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
         list(ex.map(_run, steps))
     lib = library_path()
+    relinked = False
     if force or steps or not lib.exists():
         tmp = lib.with_suffix(".so.tmp")
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-ccbin", HOST_CXX,
               "-o", str(tmp), *map(str, objs)])
         shutil.move(str(tmp), str(lib))
+        relinked = True
+    src6, obj6, lib6 = CSRC / "sapporo6thlib.cpp", BUILD / "sapporo6thlib.cpp.o", LIBDIR / LIB6TH
+    if force or _stale(obj6, src6, deps):
+        _run([HOST_CXX, *CXX_FLAGS, "-c", str(src6), "-o", str(obj6)])
+        relinked = True
+    if relinked or not lib6.exists():
+        _run([HOST_CXX, "-shared", "-o", str(lib6), str(obj6), f"-L{LIBDIR}", "-lsapporo_b200",
+              "-Wl,-rpath,$ORIGIN"])
     if verbose:
         print(f"built {lib}")
     return lib
