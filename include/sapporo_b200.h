@@ -152,6 +152,36 @@ int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, 
  * and retrieve_j_particle_state (lib/src/sapporohostclass.cpp:969-1147). */
 int sapb_read_j(sapb_dev *d, int first, int n, double ti, int predict, double *out);
 
+/* ---- Batched force evaluation: many independent force calls in one
+ * persistent launch inside a captured CUDA graph.  Replaces the reference's
+ * one-launch-per-256-i loop (lib/src/sapporohostclass.cpp:1499-1598) for
+ * block-timestep steps with uneven active counts and for ensembles of
+ * independent clusters.  A cluster is a contiguous, address-ordered range
+ * of j addresses [j_first, j_first + j_count) of this device's j store, with
+ * its own prediction time and softening, and i_count active i records
+ * (layout of sapb_i_stage) stored consecutively, cluster after cluster, in
+ * sapb_batch_i_stage().  Self pairs are skipped by id within a cluster. */
+typedef struct sapb_batch sapb_batch;
+int sapb_batch_create(sapb_dev *d, int max_clusters, int max_i, sapb_batch **out);
+int sapb_batch_destroy(sapb_batch *b);
+/* pinned i-record staging for max_i records */
+double *sapb_batch_i_stage(sapb_batch *b);
+/* Work plan of the next run: threads per i and j-split per cluster (the
+ * planner's rule, shifted by sapb_batch_set_tuning), work items in
+ * longest-first order. */
+int sapb_batch_plan(sapb_batch *b, int n_clusters, const int *j_first, const int *j_count,
+                    const int *i_count, const double *t_pred, const double *eps2);
+/* Asynchronous run: one H2D copy, one graph launch (queue reset, list-count
+ * reset, per-cluster predictor if SAPB_F_PREDICT, persistent force kernel,
+ * slice reduction), one D2H copy of the results. */
+int sapb_batch_run(sapb_batch *b, int flags);
+/* Waits; results in i-record order, SAPB_RES_STRIDE doubles each. */
+int sapb_batch_results(sapb_batch *b, const double **results, int *total_i);
+int sapb_batch_ngb_fetch(sapb_batch *b, int *counts, int *lists);
+int sapb_batch_info(sapb_batch *b, int *n_items, int *force_blocks, int *graph_runs);
+/* Autotuner knob: log2 factor on the threads-per-i rule (-5..5). */
+int sapb_batch_set_tuning(sapb_batch *b, int tpi_scale);
+
 /* Launch-shape override for the force kernel: threads per i (1,2,4,8,16,32),
  * i per thread (1,2) and j slices (>= 1).  Zeros restore the built-in
  * planner.  Replaces the compile-time NTHREADS / NBLOCKS_PER_MULTI tables

@@ -90,6 +90,15 @@ _SIGS = [
     ("sapb_read_j", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _dp]),
     ("sapb_set_launch", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     ("sapb_get_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 3),
+    ("sapb_batch_create", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("sapb_batch_destroy", C.c_int, [C.c_void_p]),
+    ("sapb_batch_i_stage", C.c_void_p, [C.c_void_p]),
+    ("sapb_batch_plan", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _ip, _dpo, _dpo]),
+    ("sapb_batch_run", C.c_int, [C.c_void_p, C.c_int]),
+    ("sapb_batch_results", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
+    ("sapb_batch_ngb_fetch", C.c_int, [C.c_void_p, _ipo, _ipo]),
+    ("sapb_batch_info", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 3),
+    ("sapb_batch_set_tuning", C.c_int, [C.c_void_p, C.c_int]),
     # class binding
     ("sapporo_c_new", C.c_void_p, []),
     ("sapporo_c_delete", None, [C.c_void_p]),
@@ -373,6 +382,72 @@ class G6:
         ovf = self.lib.g6_get_neighbour_list_(self._i(cluster), self._i(ipipe),
                                               self._i(maxlength), C.byref(n), buf)
         return ovf, n.value, buf[:min(n.value, maxlength, NGB_PB)].copy()
+
+
+class Batch:
+    """Batched force evaluation (sapb_batch_*): many clusters -- independent
+    systems or the active set of a block step -- in one persistent launch
+    replayed from a captured CUDA graph.  Clusters are contiguous,
+    address-ordered j ranges of the device's j store (set through the
+    owning :class:`Sapporo`)."""
+
+    def __init__(self, owner: "Sapporo", max_clusters: int, max_i: int):
+        self.lib, self.owner = owner.lib, owner
+        self.order = owner.order
+        self.stride = 12 if self.order >= SIXTH else 8
+        self.max_i = max_i
+        h = C.c_void_p()
+        _check(self.lib.sapb_batch_create(owner.dev, max_clusters, max_i, C.byref(h)),
+               "batch_create", owner.dev)
+        self.h = h
+        ptr = self.lib.sapb_batch_i_stage(self.h)
+        buf = (C.c_double * (max_i * self.stride)).from_address(ptr)
+        self.i_stage = np.ctypeslib.as_array(buf).reshape(max_i, self.stride)
+
+    def close(self):
+        if self.h:
+            self.lib.sapb_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def plan(self, j_first, j_count, i_count, t_pred=None, eps2=None):
+        n = len(j_first)
+        _check(self.lib.sapb_batch_plan(self.h, n, _i32(j_first), _i32(j_count), _i32(i_count),
+                                        _f64(t_pred), _f64(eps2)), "batch_plan", self.owner.dev)
+        self.total_i = int(np.sum(i_count))
+
+    def run(self, flags=F_PREDICT):
+        _check(self.lib.sapb_batch_run(self.h, int(flags)), "batch_run", self.owner.dev)
+
+    def results(self) -> np.ndarray:
+        p, n = C.c_void_p(), C.c_int()
+        _check(self.lib.sapb_batch_results(self.h, C.byref(p), C.byref(n)), "batch_results",
+               self.owner.dev)
+        if n.value == 0:
+            return np.zeros((0, RES_STRIDE))
+        buf = (C.c_double * (n.value * RES_STRIDE)).from_address(p.value)
+        return np.ctypeslib.as_array(buf).reshape(n.value, RES_STRIDE).copy()
+
+    def neighbours(self):
+        n = self.total_i
+        cnt = np.zeros(max(n, 1), dtype=np.int32)
+        lst = np.zeros(max(n, 1) * NGB_PB, dtype=np.int32)
+        _check(self.lib.sapb_batch_ngb_fetch(self.h, cnt, lst), "batch_ngb", self.owner.dev)
+        return cnt[:n], lst[:n * NGB_PB].reshape(n, NGB_PB)
+
+    def info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.sapb_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "info",
+               self.owner.dev)
+        return {"items": a.value, "force_blocks": b.value, "runs": c.value}
+
+    def set_tuning(self, tpi_scale: int):
+        _check(self.lib.sapb_batch_set_tuning(self.h, int(tpi_scale)), "tuning", self.owner.dev)
 
 
 def pack_i_records(order, x, v, h2, ids, a=None) -> np.ndarray:

@@ -8,52 +8,23 @@
 #include <new>
 
 #include "../../include/sapporo_b200.h"
+#include "sapb_dev.h"
 #include "sapb_launch.h"
 
 using namespace sapb;
 
-struct sapb_dev {
-  int device = 0;
-  int order = FOURTH;
-  int prec = DOUBLESINGLE;
-  int n_pipes = SAPB_NPIPES;
-  int num_sms = 0;
-  cudaStream_t own_stream = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
-
-  // j state
-  int cap = 0;
-  JState js{};
-  void *pred = nullptr;
-  double *jpool = nullptr;  // one allocation holding the FP64 planes
-  int *jid = nullptr;
-
-  // j staging
-  double *stage_h = nullptr;
-  double *stage_d = nullptr;
-  int stage_cap = 0;
-
-  // i records, results
-  double *irec_h = nullptr, *irec_d = nullptr;
-  int i_cap = 0;
-  double *res_h = nullptr, *res_d = nullptr;
-  int *ngb_count_d = nullptr, *ngb_list_d = nullptr;
-  double *part_d = nullptr;
-  size_t part_cap = 0;  // doubles
-  int *status_d = nullptr, *status_h = nullptr;
-  int last_ni = 0;
-  bool pending = false;
-
-  // launch overrides (0 = planner)
-  int tpi = 0, ip = 0, nslices = 0;
-
-  char err[512] = {0};
-};
-
 static char g_err[512];
 
 static int fail(sapb_dev *d, int code, const char *fmt, ...) {
+  char *buf = d ? d->err : g_err;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int sapb_fail(sapb_dev *d, int code, const char *fmt, ...) {
   char *buf = d ? d->err : g_err;
   va_list ap;
   va_start(ap, fmt);

@@ -75,6 +75,45 @@ struct ForceArgs {
   int *status;        // device error word
 };
 
+// ---- batched execution (block steps, ensembles of independent clusters) ----
+// A cluster is a contiguous range of j addresses with its own prediction time
+// and softening, plus a contiguous range of active i records.  Work items
+// (cluster, i-tile, j-slice) are consumed by a persistent kernel from a queue
+// in device memory, so one captured CUDA graph serves any step.
+struct BatchCluster {
+  int j_first, j_count;  // j addresses [j_first, j_first + j_count)
+  int i_first, i_count;  // i records [i_first, i_first + i_count)
+  int nslices;           // j-split of this cluster (1: items write results directly)
+  int part_base;         // first partial record of this cluster
+  double t_pred, eps2;
+};
+struct BatchItem {
+  int cluster;
+  int i_begin, i_count;  // global i records of this tile
+  int j_begin, j_count;  // j addresses of this slice
+  int tpi;               // threads per i (1..32), i per thread is 2
+  int slot;              // first partial record (-1: write final results)
+};
+struct BatchParams {
+  int n_items, n_clusters, total_i, j_extent;
+  int queue_head;        // next work item (reset to 0 before every run)
+  int pad[3];
+};
+struct BatchArgs {
+  const void *pred;
+  JState js;
+  void *pred_w;
+  const BatchCluster *cl;
+  const BatchItem *items;
+  BatchParams *par;
+  const double *irec;
+  double *res;
+  double *part;
+  int *ngb_count, *ngb_list;
+  int do_list, do_predict;
+  int *status;
+};
+
 struct ReduceArgs {
   const double *part;
   int nslices;

@@ -4,6 +4,7 @@
 
 #include "sapb_kernels.cuh"
 #include "sapb_launch.h"
+#include "sapb_pair.cuh"
 
 namespace sapb {
 
@@ -13,29 +14,6 @@ namespace sapb {
 // for (reference: dev_copy_particles seeds Ppos/Pvel/Pacc,
 // kernels.cu:281-297).
 // ========================================================================
-template <int ORDER, int PREC>
-__device__ __forceinline__ void store_record(void *pred, int k, double px, double py, double pz,
-                                             double m, int id, double vx, double vy, double vz,
-                                             double ax, double ay, double az) {
-  if (PREC == DOUBLE) {
-    double4 *r = reinterpret_cast<double4 *>(pred) + (size_t)k * pred_fields64(ORDER);
-    r[0] = make_double4(px, py, pz, m);
-    r[1] = make_double4(vx, vy, vz, __hiloint2double(0, id));
-    if (ORDER >= SIXTH) r[2] = make_double4(ax, ay, az, 0.0);
-  } else {
-    // Double-single split of the position: hi = (float)x, lo = (float)(x - hi)
-    // (the DSX assignment of kernels.cu:163-167).
-    const float hx = (float)px, hy = (float)py, hz = (float)pz;
-    const float lx = (float)(px - (double)hx), ly = (float)(py - (double)hy),
-                lz = (float)(pz - (double)hz);
-    float4 *r = reinterpret_cast<float4 *>(pred) + (size_t)k * pred_fields(ORDER);
-    r[0] = make_float4(hx, hy, hz, (float)m);
-    r[1] = make_float4(lx, ly, lz, __int_as_float(id));
-    r[2] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
-    if (ORDER >= SIXTH) r[3] = make_float4((float)ax, (float)ay, (float)az, 0.f);
-  }
-}
-
 template <int ORDER, int PREC>
 __global__ void __launch_bounds__(256) scatter_kernel(const double *__restrict__ stage, int n,
                                                       int cap, JState js, void *pred,
@@ -74,31 +52,6 @@ __global__ void __launch_bounds__(256) scatter_kernel(const double *__restrict__
 // Reads the FP64 structure-of-arrays state with one coalesced 8-byte load
 // per component and writes the force record of each j.
 // ========================================================================
-template <int ORDER>
-__device__ __forceinline__ void taylor(const JState &js, int k, double ti, double p[3],
-                                       double v[3], double a[3]) {
-  const double dt = ti - __ldg(js.t + k);
-  const double dt2 = (1. / 2.) * dt;
-  const double dt3 = (1. / 3.) * dt;
-  const double dt4 = (1. / 4.) * dt;
-  const double dt5 = (1. / 5.) * dt;
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const double x = __ldg(js.x[d] + k), vv = __ldg(js.v[d] + k);
-    const double aa = __ldg(js.a[d] + k), jj = __ldg(js.j[d] + k);
-    if (ORDER >= SIXTH) {
-      const double ss = __ldg(js.s[d] + k), cc = __ldg(js.c[d] + k);
-      p[d] = x + dt * (vv + dt2 * (aa + dt3 * (jj + dt4 * (ss + dt5 * (cc)))));
-      v[d] = vv + dt * (aa + dt2 * (jj + dt3 * (ss + dt4 * (cc))));
-      a[d] = aa + dt * (jj + dt2 * (ss + dt3 * (cc)));
-    } else {
-      p[d] = x + dt * (vv + dt2 * (aa + dt3 * (jj)));
-      v[d] = vv + dt * (aa + dt2 * (jj));
-      a[d] = aa;
-    }
-  }
-}
-
 template <int ORDER, int PREC>
 __global__ void __launch_bounds__(256) predict_kernel(int nj, double ti, JState js, void *pred) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -174,307 +127,6 @@ __global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti,
 // after the loop.  Rescans recompute ds2 bit-identically (same rounded
 // operations).
 // ========================================================================
-constexpr int kBT = 128;
-constexpr int kTJ = 128;
-constexpr int kNS = 3;
-
-template <int ORDER, int PREC, int TPI, int IP>
-struct FCfg {
-  static constexpr int TIT = kBT / TPI;
-  static constexpr int TI = TIT * IP;
-  static constexpr int FB = PREC == DOUBLE ? 32 : 16;
-  static constexpr int RS = PREC == DOUBLE ? pred_fields64(ORDER) : pred_fields(ORDER);
-  static constexpr int REC = RS * FB;
-  static constexpr int TILE_BYTES = kTJ * REC;
-  static constexpr int RED_BYTES = TPI > 1 ? kBT * IP * kResStride * 8 : 0;
-  static constexpr int BODY = kNS * TILE_BYTES > RED_BYTES ? kNS * TILE_BYTES : RED_BYTES;
-  // mixed precision keeps its FP64 running totals in shared memory (10 per
-  // i, [field][thread] so a warp's accesses are consecutive), which frees
-  // 40 registers per thread and lets 4 blocks share an SM
-  static constexpr int TOT_BYTES = PREC == DOUBLE ? 0 : IP * 10 * kBT * 8;
-  static constexpr int SMEM = 128 + BODY + TOT_BYTES;
-  static constexpr int MIN_BLOCKS = PREC == DOUBLE ? 1 : (IP >= 4 ? 2 : 4);
-};
-
-// ---------------- mixed precision pair ----------------
-// dr = (xj_hi - xi_hi) + (xj_lo - xi_lo) in FP32 (the double-single
-// difference of kernels.cu:169-177), everything after it in FP32 with rsqrt
-// on the MUFU pipe.  (A variant taking the difference in FP64 and rounding
-// once moved 9 FMA-pipe operations per pair to the FP64 and XU pipes but was
-// not faster: 3 FP64->FP32 conversions cost 24 XU cycles per warp and pair.)
-struct IMix {
-  float xh, yh, zh, xl, yl, zl, vx, vy, vz, ax, ay, az, h2;
-  int id;
-};
-struct AccMix {
-  float ax, ay, az, pot, jx, jy, jz, sx, sy, sz;
-};
-
-__device__ __forceinline__ float ds_sub(float jh, float jl, float ih, float il) {
-  return __fadd_rn(__fsub_rn(jh, ih), __fsub_rn(jl, il));
-}
-// dr and ds2 of one pair, self pair masked; identical in the pair loop and
-// in the rescans (explicitly rounded operations, no contraction freedom).
-__device__ __forceinline__ float pair_dr_mix(const IMix &I, const float4 &r0, const float4 &r1,
-                                             float &dx, float &dy, float &dz) {
-  dx = ds_sub(r0.x, r1.x, I.xh, I.xl);
-  dy = ds_sub(r0.y, r1.y, I.yh, I.yl);
-  dz = ds_sub(r0.z, r1.z, I.zh, I.zl);
-  dx = (__float_as_int(r1.w) == I.id) ? 1.0e18f : dx;
-  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-}
-
-template <int ORDER>
-__device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const float4 &r1,
-                                         const float4 &r2, const float4 &r3, float eps2,
-                                         AccMix &A, float &tmin) {
-  float dx, dy, dz;
-  const float ds2 = pair_dr_mix(I, r0, r1, dx, dy, dz);
-  tmin = fminf(tmin, ds2);
-  const float inv = rsqrt_mufu(ds2 + eps2);
-  const float inv2 = inv * inv;
-  const float minv = r0.w * inv;
-  const float minv3 = minv * inv2;
-  A.ax = fmaf(minv3, dx, A.ax);
-  A.ay = fmaf(minv3, dy, A.ay);
-  A.az = fmaf(minv3, dz, A.az);
-  A.pot -= minv;
-  const float dvx = r2.x - I.vx, dvy = r2.y - I.vy, dvz = r2.z - I.vz;
-  const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
-  const float m3i2 = -3.0f * inv2;
-  if (ORDER == FOURTH) {
-    // jerk += m/r^3 dv - 3 m/r^5 (dr.dv) dr   (kernels.cu:631-637)
-    const float c = (m3i2 * minv3) * rv;
-    A.jx = fmaf(c, dx, fmaf(minv3, dvx, A.jx));
-    A.jy = fmaf(c, dy, fmaf(minv3, dvy, A.jy));
-    A.jz = fmaf(c, dz, fmaf(minv3, dvz, A.jz));
-  } else {
-    // kernels.cu:642-667 with a3 = -3 alpha, b3 = -3 beta:
-    //   jerk_ij = minv3 (dv + a3 dr)
-    //   snap   += minv3 (da + b3 dr) + 2 a3 jerk_ij
-    const float dax = r3.x - I.ax, day = r3.y - I.ay, daz = r3.z - I.az;
-    const float s = fmaf(dz, daz, fmaf(dy, day, fmaf(dx, dax, fmaf(dvz, dvz, fmaf(dvy, dvy, dvx * dvx)))));
-    const float a3 = m3i2 * rv;
-    const float b3 = fmaf(a3, a3 * (-1.0f / 3.0f), s * m3i2);
-    const float c6 = (a3 + a3) * minv3;
-    const float tx = fmaf(a3, dx, dvx), ty = fmaf(a3, dy, dvy), tz = fmaf(a3, dz, dvz);
-    A.jx = fmaf(minv3, tx, A.jx);
-    A.jy = fmaf(minv3, ty, A.jy);
-    A.jz = fmaf(minv3, tz, A.jz);
-    const float ux = fmaf(b3, dx, dax), uy = fmaf(b3, dy, day), uz = fmaf(b3, dz, daz);
-    A.sx = fmaf(c6, tx, fmaf(minv3, ux, A.sx));
-    A.sy = fmaf(c6, ty, fmaf(minv3, uy, A.sy));
-    A.sz = fmaf(c6, tz, fmaf(minv3, uz, A.sz));
-  }
-}
-
-// ---------------- mixed precision, two i per thread, packed FP32x2 -------
-// The two i-particles of a thread travel in the .x/.y halves of float2
-// registers and every FP32 step is one sm_100 packed instruction
-// (__fadd2_rn / __fmul2_rn / __ffma2_rn) for both; j operands are
-// broadcast.  Per half the rounding is exactly that of the scalar path, so
-// ds2 here is bit-identical to pair_dr_mix (used by the rescans).
-struct IMix2 {
-  float2 nxh, nyh, nzh, nxl, nyl, nzl;  // negated hi / lo position parts
-  float2 nvx, nvy, nvz, nax, nay, naz;  // negated velocity, acceleration
-  int ida, idb;
-};
-struct AccMix2 {
-  float2 ax, ay, az, pot, jx, jy, jz, sx, sy, sz;  // pot accumulates +m/r
-};
-
-__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
-__device__ __forceinline__ float2 neg2(float a, float b) { return make_float2(-a, -b); }
-
-__device__ __forceinline__ IMix2 pack_i2(const IMix &a, const IMix &b) {
-  IMix2 I;
-  I.nxh = neg2(a.xh, b.xh); I.nyh = neg2(a.yh, b.yh); I.nzh = neg2(a.zh, b.zh);
-  I.nxl = neg2(a.xl, b.xl); I.nyl = neg2(a.yl, b.yl); I.nzl = neg2(a.zl, b.zl);
-  I.nvx = neg2(a.vx, b.vx); I.nvy = neg2(a.vy, b.vy); I.nvz = neg2(a.vz, b.vz);
-  I.nax = neg2(a.ax, b.ax); I.nay = neg2(a.ay, b.ay); I.naz = neg2(a.az, b.az);
-  I.ida = a.id;
-  I.idb = b.id;
-  return I;
-}
-
-template <int ORDER>
-__device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, const float4 &r1,
-                                          const float4 &r2, const float4 &r3, float2 eps2,
-                                          AccMix2 &A, float2 &tmin) {
-  // x - y == x + (-y) exactly, so these equal ds_sub of the scalar path
-  float2 dx = __fadd2_rn(__fadd2_rn(bc2(r0.x), I.nxh), __fadd2_rn(bc2(r1.x), I.nxl));
-  const float2 dy = __fadd2_rn(__fadd2_rn(bc2(r0.y), I.nyh), __fadd2_rn(bc2(r1.y), I.nyl));
-  const float2 dz = __fadd2_rn(__fadd2_rn(bc2(r0.z), I.nzh), __fadd2_rn(bc2(r1.z), I.nzl));
-  const int idj = __float_as_int(r1.w);
-  dx.x = (idj == I.ida) ? 1.0e18f : dx.x;
-  dx.y = (idj == I.idb) ? 1.0e18f : dx.y;
-  const float2 ds2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-  tmin.x = fminf(tmin.x, ds2.x);
-  tmin.y = fminf(tmin.y, ds2.y);
-  const float2 r2v = __fadd2_rn(ds2, eps2);
-  const float2 inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
-  const float2 inv2 = __fmul2_rn(inv, inv);
-  const float2 minv = __fmul2_rn(bc2(r0.w), inv);
-  const float2 minv3 = __fmul2_rn(minv, inv2);
-  A.ax = __ffma2_rn(minv3, dx, A.ax);
-  A.ay = __ffma2_rn(minv3, dy, A.ay);
-  A.az = __ffma2_rn(minv3, dz, A.az);
-  A.pot = __fadd2_rn(A.pot, minv);
-  const float2 dvx = __fadd2_rn(bc2(r2.x), I.nvx);
-  const float2 dvy = __fadd2_rn(bc2(r2.y), I.nvy);
-  const float2 dvz = __fadd2_rn(bc2(r2.z), I.nvz);
-  const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
-  const float2 m3i2 = __fmul2_rn(bc2(-3.0f), inv2);
-  if (ORDER == FOURTH) {
-    const float2 c = __fmul2_rn(__fmul2_rn(m3i2, minv3), rv);
-    A.jx = __ffma2_rn(c, dx, __ffma2_rn(minv3, dvx, A.jx));
-    A.jy = __ffma2_rn(c, dy, __ffma2_rn(minv3, dvy, A.jy));
-    A.jz = __ffma2_rn(c, dz, __ffma2_rn(minv3, dvz, A.jz));
-  } else {
-    const float2 dax = __fadd2_rn(bc2(r3.x), I.nax);
-    const float2 day = __fadd2_rn(bc2(r3.y), I.nay);
-    const float2 daz = __fadd2_rn(bc2(r3.z), I.naz);
-    const float2 s = __ffma2_rn(dz, daz, __ffma2_rn(dy, day, __ffma2_rn(dx, dax,
-                     __ffma2_rn(dvz, dvz, __ffma2_rn(dvy, dvy, __fmul2_rn(dvx, dvx))))));
-    const float2 a3 = __fmul2_rn(m3i2, rv);
-    const float2 b3 = __ffma2_rn(a3, __fmul2_rn(a3, bc2(-1.0f / 3.0f)), __fmul2_rn(s, m3i2));
-    const float2 c6 = __fmul2_rn(__fadd2_rn(a3, a3), minv3);
-    const float2 tx = __ffma2_rn(a3, dx, dvx), ty = __ffma2_rn(a3, dy, dvy),
-                 tz = __ffma2_rn(a3, dz, dvz);
-    A.jx = __ffma2_rn(minv3, tx, A.jx);
-    A.jy = __ffma2_rn(minv3, ty, A.jy);
-    A.jz = __ffma2_rn(minv3, tz, A.jz);
-    const float2 ux = __ffma2_rn(b3, dx, dax), uy = __ffma2_rn(b3, dy, day),
-                 uz = __ffma2_rn(b3, dz, daz);
-    A.sx = __ffma2_rn(c6, tx, __ffma2_rn(minv3, ux, A.sx));
-    A.sy = __ffma2_rn(c6, ty, __ffma2_rn(minv3, uy, A.sy));
-    A.sz = __ffma2_rn(c6, tz, __ffma2_rn(minv3, uz, A.sz));
-  }
-}
-
-// ---------------- FP64 pair ----------------
-struct IDp {
-  double x, y, z, vx, vy, vz, ax, ay, az, h2;
-  int id;
-};
-struct AccDp {
-  double ax, ay, az, pot, jx, jy, jz, sx, sy, sz;
-};
-
-__device__ __forceinline__ double pair_dr_dp(const IDp &I, const double4 &r0, const double4 &r1,
-                                             double &dx, double &dy, double &dz) {
-  dx = __dsub_rn(r0.x, I.x);
-  dy = __dsub_rn(r0.y, I.y);
-  dz = __dsub_rn(r0.z, I.z);
-  dx = (__double2loint(r1.w) == I.id) ? 1.0e150 : dx;
-  return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
-}
-
-template <int ORDER>
-__device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const double4 &r1,
-                                        const double4 &r2, double eps2, AccDp &A, double &tmin) {
-  double dx, dy, dz;
-  const double ds2 = pair_dr_dp(I, r0, r1, dx, dy, dz);
-  tmin = fmin(tmin, ds2);
-  const double inv = rsqrt(ds2 + eps2);
-  const double minvr1 = r0.w * inv;
-  const double invr2 = inv * inv;
-  const double minvr3 = minvr1 * invr2;
-  A.ax += minvr3 * dx;
-  A.ay += minvr3 * dy;
-  A.az += minvr3 * dz;
-  A.pot += -minvr1;
-  const double dvx = r1.x - I.vx, dvy = r1.y - I.vy, dvz = r1.z - I.vz;
-  const double rv = dx * dvx + dy * dvy + dz * dvz;
-  if (ORDER == FOURTH) {
-    const double drdv = (-3.0) * (minvr3 * invr2) * rv;
-    A.jx += minvr3 * dvx + drdv * dx;
-    A.jy += minvr3 * dvy + drdv * dy;
-    A.jz += minvr3 * dvz + drdv * dz;
-  } else {
-    const double dax = r2.x - I.ax, day = r2.y - I.ay, daz = r2.z - I.az;
-    const double v2 = dvx * dvx + dvy * dvy + dvz * dvz;
-    const double ra = dx * dax + dy * day + dz * daz;
-    double alpha = rv * invr2;
-    double beta = (v2 + ra) * invr2 + alpha * alpha;
-    alpha *= -3.0;
-    const double ex = minvr3 * dvx + alpha * (minvr3 * dx);
-    const double ey = minvr3 * dvy + alpha * (minvr3 * dy);
-    const double ez = minvr3 * dvz + alpha * (minvr3 * dz);
-    alpha *= 2.0;
-    beta *= -3.0;
-    A.sx += minvr3 * dax + alpha * ex + beta * (minvr3 * dx);
-    A.sy += minvr3 * day + alpha * ey + beta * (minvr3 * dy);
-    A.sz += minvr3 * daz + alpha * ez + beta * (minvr3 * dz);
-    A.jx += ex;
-    A.jy += ey;
-    A.jz += ez;
-  }
-}
-
-__device__ __forceinline__ void list_push(int *cnt, int *list, int gi, int idj) {
-  const int pos = atomicAdd(cnt + gi, 1);
-  if (pos < kNgbPB) list[(size_t)gi * kNgbPB + pos] = idj;
-}
-
-// Warp-cooperative neighbour-list rescan of one shared-memory tile: for every
-// lane whose i saw a pair below h2 in this tile, the whole warp re-evaluates
-// that i against the tile's j (lane-strided) and appends the hits.
-template <int PREC, int RS, int TPI>
-__device__ __forceinline__ void list_rescan_mix(const IMix &I, bool want, int gi, int row,
-                                                const float4 *rec, int cnt, int lane,
-                                                int *ngb_count, int *ngb_list) {
-  unsigned m = __ballot_sync(0xffffffffu, want);
-  while (m) {
-    const int src = __ffs(m) - 1;
-    m &= m - 1;
-    IMix S;
-    S.xh = __shfl_sync(0xffffffffu, I.xh, src);
-    S.yh = __shfl_sync(0xffffffffu, I.yh, src);
-    S.zh = __shfl_sync(0xffffffffu, I.zh, src);
-    S.xl = __shfl_sync(0xffffffffu, I.xl, src);
-    S.yl = __shfl_sync(0xffffffffu, I.yl, src);
-    S.zl = __shfl_sync(0xffffffffu, I.zl, src);
-    S.h2 = __shfl_sync(0xffffffffu, I.h2, src);
-    S.id = __shfl_sync(0xffffffffu, I.id, src);
-    const int sgi = __shfl_sync(0xffffffffu, gi, src);
-    const int srow = __shfl_sync(0xffffffffu, row, src);
-    for (int k = srow + lane * TPI; k < cnt; k += 32 * TPI) {
-      float dx, dy, dz;
-      const float4 r0 = rec[k * RS + 0];
-      const float4 r1 = rec[k * RS + 1];
-      const float ds2 = pair_dr_mix(S, r0, r1, dx, dy, dz);
-      if (ds2 < S.h2) list_push(ngb_count, ngb_list, sgi, __float_as_int(r1.w));
-    }
-  }
-}
-
-template <int PREC, int RS, int TPI>
-__device__ __forceinline__ void list_rescan_dp(const IDp &I, bool want, int gi, int row,
-                                               const double4 *rec, int cnt, int lane,
-                                               int *ngb_count, int *ngb_list) {
-  unsigned m = __ballot_sync(0xffffffffu, want);
-  while (m) {
-    const int src = __ffs(m) - 1;
-    m &= m - 1;
-    IDp S;
-    S.x = __shfl_sync(0xffffffffu, I.x, src);
-    S.y = __shfl_sync(0xffffffffu, I.y, src);
-    S.z = __shfl_sync(0xffffffffu, I.z, src);
-    S.h2 = __shfl_sync(0xffffffffu, I.h2, src);
-    S.id = __shfl_sync(0xffffffffu, I.id, src);
-    const int sgi = __shfl_sync(0xffffffffu, gi, src);
-    const int srow = __shfl_sync(0xffffffffu, row, src);
-    for (int k = srow + lane * TPI; k < cnt; k += 32 * TPI) {
-      double dx, dy, dz;
-      const double4 r0 = rec[k * RS + 0];
-      const double4 r1 = rec[k * RS + 1];
-      const double ds2 = pair_dr_dp(S, r0, r1, dx, dy, dz);
-      if (ds2 < S.h2) list_push(ngb_count, ngb_list, sgi, __double2loint(r1.w));
-    }
-  }
-}
-
 template <int ORDER, int PREC, int TPI, int IP>
 __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
     force_kernel(ForceArgs A) {
@@ -605,8 +257,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           best_tile[p] = it;
         }
         if (A.do_list)
-          list_rescan_dp<PREC, C::RS, TPI>(Id[p], tmin[p] < Id[p].h2, gi[p], ty, rec, cnt, lane,
-                                           A.ngb_count, A.ngb_list);
+          list_rescan_dp<C::RS>(Id[p], tmin[p] < Id[p].h2, gi[p], ty, TPI, rec, cnt, lane,
+                                A.ngb_count, A.ngb_list);
       }
     } else {
       const float4 *rec = reinterpret_cast<const float4 *>(buf);
@@ -676,8 +328,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           best_tile[p] = it;
         }
         if (A.do_list)
-          list_rescan_mix<PREC, C::RS, TPI>(Im[p], tmin[p] < Im[p].h2, gi[p], ty, rec, cnt, lane,
-                                            A.ngb_count, A.ngb_list);
+          list_rescan_mix<C::RS>(Im[p], tmin[p] < Im[p].h2, gi[p], ty, TPI, rec, cnt, lane,
+                                 A.ngb_count, A.ngb_list);
       }
     }
     __syncwarp();
