@@ -222,6 +222,101 @@ def cpu_baseline_leg(cfg, nsample: int):
             "interactions": inter}
 
 
+def ensemble_inputs(k: int, seed: int):
+    """512-cluster ensemble: N_c ~ logU[256, 16384], own t_i, active fraction
+    ~ logU[1/N_c, 1], 4th order.  j acc/jerk from an FP64 direct sum done by
+    one batched FP64 run over all clusters."""
+    import sapporo2_b200 as sp
+    from sapporo2_b200 import ic
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(256), np.log(16384), k)).astype(int)
+    cl = []
+    for c, n in enumerate(ns):
+        x, v, m = ic.plummer(int(n), seed * 1000 + c)
+        ti = 1.0 + 0.01 * c
+        t0 = ti - rng.integers(0, 8, n) * 2.0 ** -10
+        frac = np.exp(rng.uniform(np.log(1.0 / n), 0.0))
+        active = np.sort(rng.choice(n, max(1, int(round(frac * n))), replace=False))
+        cl.append({"n": int(n), "x": x, "v": v, "m": m, "ti": ti, "t0": t0, "active": active,
+                   "id": np.arange(n, dtype=np.int32), "eps2": 1e-6})
+    total = int(ns.sum())
+    first = np.concatenate([[0], np.cumsum(ns)[:-1]]).astype(np.int32)
+    # derivatives: every particle of every cluster active, no prediction, FP64
+    z = np.zeros((total, 3))
+    X = np.concatenate([c["x"] for c in cl])
+    V = np.concatenate([c["v"] for c in cl])
+    M = np.concatenate([c["m"] for c in cl])
+    ID = np.concatenate([c["id"] for c in cl])
+    with sp.Sapporo(order=sp.FOURTH, precision=sp.DOUBLE) as s:
+        s.set_j_particles(np.arange(total), ID, np.zeros(total), M, X, V, z, z)
+        s.force_prediction(total)
+        with sp.Batch(s, k, total) as b:
+            b.plan(first, ns, ns, np.zeros(k), np.full(k, 1e-6))
+            b.i_stage[:total] = sp.pack_i_records(1, X, V, None, ID)
+            b.run(0)
+            r = b.results()
+    A, J = r[:, 0:3], r[:, 4:7]
+    for c, f in zip(cl, first):
+        c["a"], c["j"] = A[f:f + c["n"]], J[f:f + c["n"]]
+        c["px"], c["pv"], _ = ic.predict_fp64(1, c["ti"], c["t0"], c["x"], c["v"], c["a"], c["j"])
+    return cl, first, ns
+
+
+def run_ensemble_bench(args, torch):
+    import sapporo2_b200 as sp
+    t_build = time.time()
+    cl, first, ns = ensemble_inputs(512, seed=4)
+    log(f"[bench] ensemble of {len(cl)} clusters, {int(ns.sum())} particles built in "
+        f"{time.time() - t_build:.1f}s")
+    total = int(ns.sum())
+    act = np.array([len(c["active"]) for c in cl])
+    inter = float(np.sum(act * ns))
+    with sp.Sapporo(order=sp.FOURTH, precision=sp.DOUBLESINGLE) as s:
+        stream = torch.cuda.Stream()
+        s.set_stream(stream.cuda_stream)
+        X = np.concatenate([c["x"] for c in cl])
+        s.set_j_particles(np.arange(total), np.concatenate([c["id"] for c in cl]),
+                          np.concatenate([c["t0"] for c in cl]), np.concatenate([c["m"] for c in cl]),
+                          X, np.concatenate([c["v"] for c in cl]),
+                          np.concatenate([c["a"] for c in cl]), np.concatenate([c["j"] for c in cl]))
+        s.force_prediction(total)
+        with sp.Batch(s, len(cl), int(act.sum())) as b:
+            b.plan(first, ns, act, [c["ti"] for c in cl], [c["eps2"] for c in cl])
+            row = 0
+            for c in cl:
+                a = c["active"]
+                b.i_stage[row:row + len(a)] = sp.pack_i_records(1, c["px"][a], c["pv"][a], None,
+                                                                c["id"][a])
+                row += len(a)
+            tune = b.autotune(sp.F_PREDICT, reps=3)
+            info = b.info()
+            times = []
+            for it in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                b.run(sp.F_PREDICT)
+                res = b.results()
+                if it >= args.warmup:
+                    times.append(time.perf_counter() - t0)
+    per = float(np.mean(times))
+    dev_ms = tune["ms"]
+    print(json.dumps({
+        "metric": "interactions/s, ensemble of 512 Plummer clusters (N~logU[256,16384], own t_i, "
+                  "active~logU[1/N,1]), Hermite 4th order mixed, one persistent launch per step",
+        "value": inter / (dev_ms * 1e-3), "unit": "interactions/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 body",
+        "data": "synthetic",
+        "config": {"workload": "ensemble (C4)", "clusters": len(cl), "particles": total,
+                   "active_i": int(act.sum()), "interactions_per_step": inter,
+                   "autotune": tune, "work_items": info["items"],
+                   "persistent_blocks": info["force_blocks"]},
+        "e2e": {"value": inter / per, "unit": "interactions/s", "s_per_step": per,
+                "h2d_bytes_per_step": int(act.sum()) * 64, "d2h_bytes_per_step": int(act.sum()) * 96,
+                "api": "sapb_batch_run + sapb_batch_results (tables, i records, graph, results)"},
+        "gpu_launches": 3 * args.steps,
+    }), flush=True)
+
+
 def rel_stats(got, want):
     e = np.linalg.norm(got - want, axis=1) / np.maximum(np.linalg.norm(want, axis=1), 1e-300)
     return {"median": float(np.median(e)), "max": float(e.max())}
@@ -282,6 +377,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["precision", "ensemble"], default="precision",
+                    help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters")
     ap.add_argument("--launch", default=None,
                     help="force-kernel shape override tpi,ip,slices (default: planner)")
     ap.add_argument("--only", choices=["all", "mixed"], default="all",
@@ -310,6 +407,9 @@ def main():
     os.environ.setdefault("CUDA_VISIBLE_DEVICES_LOCAL", str(local))
 
     import sapporo2_b200 as sp
+    if args.workload == "ensemble":
+        run_ensemble_bench(args, torch)
+        return
     n = args.n
     cfg = build_inputs(n, seed=3 + rank)
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")

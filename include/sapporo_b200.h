@@ -181,6 +181,11 @@ int sapb_batch_ngb_fetch(sapb_batch *b, int *counts, int *lists);
 int sapb_batch_info(sapb_batch *b, int *n_items, int *force_blocks, int *graph_runs);
 /* Autotuner knob: log2 factor on the threads-per-i rule (-5..5). */
 int sapb_batch_set_tuning(sapb_batch *b, int tpi_scale);
+/* Measures the last plan's workload under each threads-per-i scale
+ * (-1..2) and j-split density (2, 4, 8 items per resident block), `reps`
+ * graph replays each, keeps the fastest and re-plans with it. */
+int sapb_batch_autotune(sapb_batch *b, int flags, int reps, int *best_scale, int *best_split,
+                        float *best_ms);
 
 /* Launch-shape override for the force kernel: threads per i (1,2,4,8,16,32),
  * i per thread (1,2) and j slices (>= 1).  Zeros restore the built-in

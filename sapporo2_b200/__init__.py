@@ -99,6 +99,8 @@ _SIGS = [
     ("sapb_batch_ngb_fetch", C.c_int, [C.c_void_p, _ipo, _ipo]),
     ("sapb_batch_info", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 3),
     ("sapb_batch_set_tuning", C.c_int, [C.c_void_p, C.c_int]),
+    ("sapb_batch_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     # class binding
     ("sapporo_c_new", C.c_void_p, []),
     ("sapporo_c_delete", None, [C.c_void_p]),
@@ -448,6 +450,12 @@ class Batch:
 
     def set_tuning(self, tpi_scale: int):
         _check(self.lib.sapb_batch_set_tuning(self.h, int(tpi_scale)), "tuning", self.owner.dev)
+
+    def autotune(self, flags=F_PREDICT, reps=2) -> dict:
+        sc, sf, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.sapb_batch_autotune(self.h, int(flags), int(reps), C.byref(sc),
+                                            C.byref(sf), C.byref(ms)), "autotune", self.owner.dev)
+        return {"tpi_scale": sc.value, "split_factor": sf.value, "ms": ms.value}
 
 
 def pack_i_records(order, x, v, h2, ids, a=None) -> np.ndarray:

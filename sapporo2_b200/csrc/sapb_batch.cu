@@ -42,8 +42,12 @@ struct sapb_batch {
   int force_blocks = 0;
   cudaEvent_t done = nullptr;
   bool pending = false;
-  int tpi_scale = 0;  // autotuner offset: log2 factor applied to the threads-per-i rule
+  int tpi_scale = 0;     // autotuner: log2 factor applied to the threads-per-i rule
+  int split_factor = 4;  // autotuner: work items per resident block targeted by the j-split
   int runs = 0;
+  // inputs of the last plan (re-planned by the autotuner)
+  std::vector<int> p_jf, p_jc, p_ic;
+  std::vector<double> p_t, p_e;
 
   BatchParams *par_h() { return reinterpret_cast<BatchParams *>(blob_h); }
   BatchCluster *cl_h() { return reinterpret_cast<BatchCluster *>(blob_h + off_cl); }
@@ -187,10 +191,10 @@ int sapb_batch_plan(sapb_batch *b, int n_clusters, const int *j_first, const int
   }
   if (i_first > b->max_i)
     return sapb_fail(d, SAPB_EINVAL, "%d active i (capacity %d)", i_first, b->max_i);
-  // j-split: aim at >= 4 items per resident block for balance; slices of at
-  // least 256 j
-  const long long target =
-      std::max<long long>(256, total_weight / std::max(1, 4 * b->force_blocks));
+  // j-split: aim at split_factor items per resident block for balance;
+  // slices of at least 256 j
+  const long long target = std::max<long long>(
+      256, total_weight / std::max(1, b->split_factor * b->force_blocks));
   int n_items = 0;
   size_t part = 0;
   for (int c = 0; c < n_clusters; c++) {
@@ -228,6 +232,15 @@ int sapb_batch_plan(sapb_batch *b, int n_clusters, const int *j_first, const int
   // longest items first
   std::stable_sort(it, it + n_items,
                    [](const BatchItem &a, const BatchItem &c) { return a.j_count > c.j_count; });
+  b->p_jf.assign(j_first, j_first + n_clusters);
+  b->p_jc.assign(j_count, j_count + n_clusters);
+  b->p_ic.assign(i_count, i_count + n_clusters);
+  b->p_t.assign(n_clusters, 0.0);
+  b->p_e.assign(n_clusters, 0.0);
+  for (int c = 0; c < n_clusters; c++) {
+    b->p_t[c] = cl[c].t_pred;
+    b->p_e[c] = cl[c].eps2;
+  }
   b->n_clusters = n_clusters;
   b->n_items = n_items;
   b->total_i = i_first;
@@ -354,6 +367,63 @@ int sapb_batch_set_tuning(sapb_batch *b, int tpi_scale) {
     return sapb_fail(b ? b->d : nullptr, SAPB_EINVAL, "tpi scale %d", tpi_scale);
   b->tpi_scale = tpi_scale;
   return SAPB_OK;
+}
+
+int sapb_batch_autotune(sapb_batch *b, int flags, int reps, int *best_scale, int *best_split,
+                        float *best_ms) {
+  if (!b || b->p_jf.empty() || reps < 1)
+    return sapb_fail(b ? b->d : nullptr, SAPB_EINVAL, "autotune needs a plan and reps >= 1");
+  sapb_dev *d = b->d;
+  BK(b, cudaSetDevice(d->device));
+  const int n = (int)b->p_jf.size();
+  const std::vector<int> jf = b->p_jf, jc = b->p_jc, ic = b->p_ic;
+  const std::vector<double> tp = b->p_t, ep = b->p_e;
+  cudaEvent_t e0, e1;
+  BK(b, cudaEventCreate(&e0));
+  BK(b, cudaEventCreate(&e1));
+  float best = 3.4e38f;
+  int bs = b->tpi_scale, bf = b->split_factor;
+  static const int scales[] = {-1, 0, 1, 2};
+  static const int splits[] = {2, 4, 8};
+  int rc = SAPB_OK;
+  for (int sc : scales) {
+    for (int sf : splits) {
+      b->tpi_scale = sc;
+      b->split_factor = sf;
+      rc = sapb_batch_plan(b, n, jf.data(), jc.data(), ic.data(), tp.data(), ep.data());
+      if (rc) break;
+      rc = sapb_batch_run(b, flags);  // warm-up (and graph capture if needed)
+      if (!rc) rc = sapb_batch_results(b, nullptr, nullptr);
+      if (rc) break;
+      if (cudaEventRecord(e0, d->stream) != cudaSuccess) { rc = SAPB_ECUDA; break; }
+      for (int r = 0; r < reps && !rc; r++)
+        if (cudaGraphLaunch(b->exec, d->stream) != cudaSuccess) rc = SAPB_ECUDA;
+      if (rc || cudaEventRecord(e1, d->stream) != cudaSuccess ||
+          cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = SAPB_ECUDA;
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= reps;
+      if (ms < best) {
+        best = ms;
+        bs = sc;
+        bf = sf;
+      }
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->tpi_scale = bs;
+  b->split_factor = bf;
+  if (rc) return sapb_fail(d, rc, "autotune: a trial run failed");
+  rc = sapb_batch_plan(b, n, jf.data(), jc.data(), ic.data(), tp.data(), ep.data());
+  if (best_scale) *best_scale = bs;
+  if (best_split) *best_split = bf;
+  if (best_ms) *best_ms = best;
+  return rc;
 }
 
 }  // extern "C"
