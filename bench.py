@@ -317,6 +317,57 @@ def run_ensemble_bench(args, torch):
     }), flush=True)
 
 
+def run_learned_h2_bench(args):
+    """The learned-h2 workload: N=262144 Plummer + 10 % binaries, 6th-order
+    block steps, neighbour lists on (target 32, cap 256), the same steps run
+    with the fixed global radius, the count-scaled radius and the learned
+    radius.  Forces do not depend on the radius, so the three trajectories
+    are identical; the policies differ in overflows, retries and time."""
+    from sapporo2_b200 import hermite6 as H, ic
+    cfg = ic.make_config("C5", n=args.c5_n, seed=5)
+    policies = {"fixed": lambda: H.FixedH2(), "count_scaled": lambda: H.CountScaledH2(),
+                "learned": lambda: (lambda sap: H.LearnedH2(sap, seed=5))}
+    out, final = {}, {}
+    for name, make in policies.items():
+        t0 = time.perf_counter()
+        sim = H.BlockHermite6(cfg["x"], cfg["v"], cfg["m"], cfg["eps2"], make())
+        t_init = time.perf_counter() - t0
+        active = []
+        for _ in range(args.c5_steps):
+            active.append(sim.step())
+        de = abs(sim.energy() - sim.e0) / abs(sim.e0)
+        st = dict(sim.stats)
+        ev = max(st["evaluated"], 1)
+        out[name] = {
+            "overflow_rate": st["overflow"] / ev, "overflows": st["overflow"],
+            "retries": st["retries"], "retry_rounds": st["rounds"],
+            "in_range_frac": st["in_range"] / ev, "evaluations": st["evaluated"],
+            "ms_per_step": 1e3 * st["step_s"] / max(st["steps"], 1),
+            "force_ms_per_step": 1e3 * st["force_s"] / max(st["steps"], 1),
+            "train_ms_per_step": 1e3 * getattr(sim.policy, "train_s", 0.0) / max(st["steps"], 1),
+            "pretrain_s": getattr(sim.policy, "pretrain_s", 0.0),
+            "init_s": t_init, "t_end": float(sim.t.max()), "rel_energy_error": de,
+            "mean_active": float(np.mean(active)),
+            "interactions_per_step": st["interactions"] / max(st["steps"], 1),
+        }
+        final[name] = (sim.x.copy(), sim.v.copy())
+        log(f"[bench] learned_h2 {name}: {out[name]}")
+        sim.close()
+    same = all(np.array_equal(final[k][0], final["fixed"][0]) and
+               np.array_equal(final[k][1], final["fixed"][1]) for k in final)
+    fr, lr_ = out["fixed"]["retries"], out["learned"]["retries"]
+    print(json.dumps({
+        "metric": "neighbour-overflow retries over the block steps, fixed global h2 / learned h2 "
+                  "(N=262144 Plummer + 10% binaries, 6th order, target 32, cap 256)",
+        "value": fr / max(lr_, 1), "unit": "x fewer retries", "n_gpus": 1,
+        "steps": args.c5_steps, "warmup": 0, "ms_per_step": out["learned"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 body, f64 corrector", "data": "synthetic",
+        "config": {"workload": "learned h2 (C5)", "n": args.c5_n, "block_steps": args.c5_steps,
+                   "identical_trajectories": bool(same), "policies": out},
+    }), flush=True)
+
+
 def rel_stats(got, want):
     e = np.linalg.norm(got - want, axis=1) / np.maximum(np.linalg.norm(want, axis=1), 1e-300)
     return {"median": float(np.median(e)), "max": float(e.max())}
@@ -377,8 +428,12 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["precision", "ensemble"], default="precision",
-                    help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters")
+    ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2"],
+                    default="precision",
+                    help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters; "
+                         "learned_h2: block steps with fixed, count-scaled and learned h2")
+    ap.add_argument("--c5-n", type=int, default=262144)
+    ap.add_argument("--c5-steps", type=int, default=200)
     ap.add_argument("--launch", default=None,
                     help="force-kernel shape override tpi,ip,slices (default: planner)")
     ap.add_argument("--only", choices=["all", "mixed"], default="all",
@@ -409,6 +464,9 @@ def main():
     import sapporo2_b200 as sp
     if args.workload == "ensemble":
         run_ensemble_bench(args, torch)
+        return
+    if args.workload == "learned_h2":
+        run_learned_h2_bench(args)
         return
     n = args.n
     cfg = build_inputs(n, seed=3 + rank)

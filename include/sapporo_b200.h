@@ -187,6 +187,28 @@ int sapb_batch_set_tuning(sapb_batch *b, int tpi_scale);
 int sapb_batch_autotune(sapb_batch *b, int flags, int reps, int *best_scale, int *best_split,
                         float *best_ms);
 
+/* ---- Neighbour-radius network (no counterpart in the reference; the
+ * reference's h2 comes from the caller).  A 5 -> 64 -> 64 -> 64 -> 1 ReLU
+ * perceptron with FP32 weights, run and trained on this device by the
+ * library's own CUDA kernels.  Host arrays: x [n][5] floats, t and y [n].
+ * Parameters: sapb_mlp_num_params() floats in the order W1[64][5] b1 W2[64][64]
+ * b2 W3[64][64] b3 W4[64] b4. */
+typedef struct sapb_mlp sapb_mlp;
+int sapb_mlp_num_params(void);
+/* He/Glorot-uniform initialisation from `seed` (splitmix64 stream). */
+int sapb_mlp_create(sapb_dev *d, unsigned long long seed, sapb_mlp **out);
+int sapb_mlp_destroy(sapb_mlp *m);
+int sapb_mlp_set_params(sapb_mlp *m, const float *params);  /* also resets Adam state */
+int sapb_mlp_get_params(sapb_mlp *m, float *params);
+/* y = net(x) for n samples (synchronous). */
+int sapb_mlp_forward(sapb_mlp *m, int n, const float *x, float *y);
+/* Gradient of 1/(2n) sum (net(x) - t)^2 (grad may be NULL) and the loss. */
+int sapb_mlp_gradient(sapb_mlp *m, int n, const float *x, const float *t, float *grad,
+                      float *loss);
+/* `epochs` full-batch Adam steps (lr, beta 0.9/0.999); loss before the last. */
+int sapb_mlp_train(sapb_mlp *m, int n, const float *x, const float *t, int epochs, float lr,
+                   float *loss);
+
 /* Launch-shape override for the force kernel: threads per i (1,2,4,8,16,32),
  * i per thread (1,2) and j slices (>= 1).  Zeros restore the built-in
  * planner.  Replaces the compile-time NTHREADS / NBLOCKS_PER_MULTI tables

@@ -101,6 +101,18 @@ _SIGS = [
     ("sapb_batch_set_tuning", C.c_int, [C.c_void_p, C.c_int]),
     ("sapb_batch_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    ("sapb_mlp_num_params", C.c_int, []),
+    ("sapb_mlp_create", C.c_int, [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    ("sapb_mlp_destroy", C.c_int, [C.c_void_p]),
+    ("sapb_mlp_set_params", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    ("sapb_mlp_get_params", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    ("sapb_mlp_forward", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float)]),
+    ("sapb_mlp_gradient", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float)]),
+    ("sapb_mlp_train", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                 C.c_int, C.c_float, C.POINTER(C.c_float)]),
     # class binding
     ("sapporo_c_new", C.c_void_p, []),
     ("sapporo_c_delete", None, [C.c_void_p]),
@@ -204,14 +216,26 @@ class Sapporo:
     """The ``sapporo`` class (C++), one GPU.  Method names follow the
     reference; array arguments are numpy arrays ([n, 3] for vectors)."""
 
-    def __init__(self, device: int = 0, order: int = FOURTH, precision: int = DOUBLESINGLE):
+    def __init__(self, device: int = 0, order: int = FOURTH, precision: int = DOUBLESINGLE,
+                 n_pipes: int | None = None):
         self.lib = load_library()
         self.h = self.lib.sapporo_c_new()
         if not self.h:
             raise SapporoError("allocation failed")
         self.order = order
         self.precision = precision
-        _check(self.lib.sapporo_c_open(self.h, device, order, precision), "open")
+        # n_pipes (max i per start) is read from SAPPORO_NPIPES at open, as in the C++ class
+        old = os.environ.get("SAPPORO_NPIPES")
+        if n_pipes:
+            os.environ["SAPPORO_NPIPES"] = str(int(n_pipes))
+        try:
+            _check(self.lib.sapporo_c_open(self.h, device, order, precision), "open")
+        finally:
+            if n_pipes:
+                if old is None:
+                    del os.environ["SAPPORO_NPIPES"]
+                else:
+                    os.environ["SAPPORO_NPIPES"] = old
         self.dev = self.lib.sapporo_c_device(self.h)
 
     def close(self):
@@ -276,6 +300,19 @@ class Sapporo:
 
     def read_ngb_list(self) -> int:
         return self.lib.sapporo_c_read_ngb_list(self.h)
+
+    def neighbour_counts(self, ni=None) -> np.ndarray:
+        """Exact neighbour counts of the last force call (the lists hold at most
+        NGB_PB ids; a count >= NGB_PB is an overflow)."""
+        ni = self._ni if ni is None else ni
+        cnt = np.zeros(max(ni, 1), dtype=np.int32)
+        self.results_ready()
+        _check(self.lib.sapb_ngb_fetch(self.dev, cnt, None, ni), "ngb_fetch", self.dev)
+        return cnt[:ni]
+
+    def results_ready(self):
+        p, n = C.c_void_p(), C.c_int()
+        _check(self.lib.sapb_results(self.dev, C.byref(p), C.byref(n)), "results", self.dev)
 
     def get_ngb_list(self, ipipe: int, maxlength: int = NGB_PB):
         buf = np.zeros(max(maxlength, 1), dtype=np.int32)

@@ -38,7 +38,8 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CSRC}",
              f"-I{CUDA_HOME / 'include'}"]
 
-CU_SOURCES = ["sapb_kernels.cu", "sapb_capi.cu", "sapb_batch_kernels.cu", "sapb_batch.cu"]
+CU_SOURCES = ["sapb_kernels.cu", "sapb_capi.cu", "sapb_batch_kernels.cu", "sapb_batch.cu",
+              "sapb_mlp.cu"]
 CXX_SOURCES = ["sapporohostclass.cpp", "sapporoG6lib.cpp", "sapporo_cbind.cpp"]
 
 

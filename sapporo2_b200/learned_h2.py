@@ -1,0 +1,142 @@
+"""Learned neighbour radius: the network of sapb_mlp.cu proposes each
+particle's h2 from five features of its previous force evaluation, and is
+trained online on the neighbour counts the force kernel reports.
+
+Features (all logarithmic, standardised with statistics frozen at the first
+training call): local density estimate n_prev / (4/3 pi h_prev^3), |a|,
+|jerk|, 1 + n_prev, h2_prev.  The proposal is
+log(h2 / h2_prev) = 2/3 log(target / n_prev) + network output: the network
+learns the correction to the count-scaled radius (density drift along the
+orbit, regression of noisy small counts).  Target for a particle evaluated
+with h2_used that found n neighbours: the radius that would have given the
+target count in a locally uniform medium,
+log(h2_used / h2_prev) + 2/3 log(target / max(n, 1/2)), minus the
+count-scaled part.
+
+The fixed rule with overflow re-evaluation (`retry_h2`) stays as the fallback
+and judge: any overflowing particle is re-evaluated with the count-scaled
+radius, so results never depend on the network.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import Sapporo, SapporoError, _check, load_library
+
+TARGET = 32.0
+CAP = 256
+
+
+def features(n_prev, h2_prev, acc, jrk) -> np.ndarray:
+    n = np.maximum(np.asarray(n_prev, dtype=np.float64), 0.5)
+    h2 = np.asarray(h2_prev, dtype=np.float64)
+    rho = n / (4.0 / 3.0 * np.pi * h2 ** 1.5)
+    a = np.linalg.norm(acc, axis=1) + 1e-30
+    j = np.linalg.norm(jrk, axis=1) + 1e-30
+    return np.stack([np.log(rho), np.log(a), np.log(j), np.log1p(n), np.log(h2)], axis=1)
+
+
+def target_log_ratio(h2_used, h2_prev, n_obs, target=TARGET) -> np.ndarray:
+    n = np.maximum(np.asarray(n_obs, dtype=np.float64), 0.5)
+    return np.log(np.asarray(h2_used) / np.asarray(h2_prev)) + (2.0 / 3.0) * np.log(target / n)
+
+
+def retry_h2(h2, count, target=TARGET) -> np.ndarray:
+    """Radius for re-evaluating an overflowing particle (exact counts)."""
+    return np.asarray(h2) * (target / np.maximum(np.asarray(count, dtype=np.float64), 1.0)) ** (2.0 / 3.0)
+
+
+class H2Net:
+    """The network on the GPU of an open :class:`Sapporo` instance."""
+
+    def __init__(self, owner: Sapporo, seed: int = 5):
+        self.lib = load_library()
+        self.owner = owner
+        self.np = self.lib.sapb_mlp_num_params()
+        h = C.c_void_p()
+        _check(self.lib.sapb_mlp_create(owner.dev, C.c_ulonglong(seed), C.byref(h)), "mlp_create",
+               owner.dev)
+        self.h = h
+        self.mu = None
+        self.sd = None
+
+    def close(self):
+        if self.h:
+            self.lib.sapb_mlp_destroy(self.h)
+            self.h = None
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.np, dtype=np.float32)
+        _check(self.lib.sapb_mlp_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))),
+               "mlp_get", self.owner.dev)
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self.lib.sapb_mlp_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))),
+               "mlp_set", self.owner.dev)
+
+    @staticmethod
+    def _f(a):
+        return np.ascontiguousarray(a, dtype=np.float32)
+
+    def forward(self, x) -> np.ndarray:
+        x = self._f(x)
+        y = np.zeros(len(x), dtype=np.float32)
+        _check(self.lib.sapb_mlp_forward(self.h, len(x), x.ctypes.data_as(C.POINTER(C.c_float)),
+                                         y.ctypes.data_as(C.POINTER(C.c_float))), "mlp_forward",
+               self.owner.dev)
+        return y
+
+    def gradient(self, x, t):
+        x, t = self._f(x), self._f(t)
+        g = np.zeros(self.np, dtype=np.float32)
+        loss = C.c_float()
+        _check(self.lib.sapb_mlp_gradient(self.h, len(x), x.ctypes.data_as(C.POINTER(C.c_float)),
+                                          t.ctypes.data_as(C.POINTER(C.c_float)),
+                                          g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)),
+               "mlp_gradient", self.owner.dev)
+        return g, loss.value
+
+    def train(self, x, t, epochs=20, lr=1e-3) -> float:
+        x, t = self._f(x), self._f(t)
+        loss = C.c_float()
+        _check(self.lib.sapb_mlp_train(self.h, len(x), x.ctypes.data_as(C.POINTER(C.c_float)),
+                                       t.ctypes.data_as(C.POINTER(C.c_float)), int(epochs),
+                                       float(lr), C.byref(loss)), "mlp_train", self.owner.dev)
+        return loss.value
+
+    # ---- standardised use -------------------------------------------------
+    def fit_standardisation(self, f, floor=0.5):
+        """Freezes the feature scaling (mean, std floored at `floor`: the
+        features are logarithms, so a constant start-up feature such as one
+        global h2 must not blow up later variations)."""
+        self.mu = f.mean(0)
+        self.sd = np.maximum(f.std(0), floor)
+
+    def standardise(self, f):
+        if self.mu is None:
+            self.fit_standardisation(f)
+        return (f - self.mu) / self.sd
+
+    @staticmethod
+    def base_log_ratio(n_prev, target=TARGET) -> np.ndarray:
+        """The count-scaled step the network corrects: log of
+        (target / previous count)^(2/3)."""
+        return (2.0 / 3.0) * np.log(target / np.maximum(np.asarray(n_prev, dtype=np.float64), 0.5))
+
+    def propose(self, n_prev, h2_prev, acc, jrk, clip=4.0) -> np.ndarray:
+        """h2 for the next evaluation: the count-scaled radius times the
+        network's correction (log-ratio clipped to +-clip)."""
+        f = self.standardise(features(n_prev, h2_prev, acc, jrk))
+        r = self.base_log_ratio(n_prev) + self.forward(f).astype(np.float64)
+        return np.asarray(h2_prev) * np.exp(np.clip(r, -clip, clip))
+
+    def learn(self, n_prev, h2_prev, acc, jrk, h2_used, n_obs, epochs=20, lr=2e-3) -> float:
+        """One online update: the correction that would have given the target
+        count, from the count the force kernel found with h2_used."""
+        f = self.standardise(features(n_prev, h2_prev, acc, jrk))
+        y = target_log_ratio(h2_used, h2_prev, n_obs) - self.base_log_ratio(n_prev)
+        return self.train(f, y, epochs, lr)

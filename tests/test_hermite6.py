@@ -1,0 +1,74 @@
+"""The block-timestep 6th-order Hermite integrator and the neighbour-radius
+policies: host logic on CPU through the FP64 oracle (energy conservation,
+overflow re-evaluation until no list overflows, forces independent of the
+radius), and the learned radius on the GPU (overflow retries against the
+fixed rule at identical step results)."""
+import numpy as np
+import pytest
+
+from sapporo2_b200 import NGB_PB, hermite6 as H, ic
+from sapporo2_b200.learned_h2 import retry_h2
+
+from tests.oracle_backend import OracleBackend
+
+
+def _cluster(n, seed=5):
+    cfg = ic.make_config("C5", n=n, seed=seed)
+    return cfg["x"], cfg["v"], cfg["m"], cfg["eps2"]
+
+
+def test_retry_radius_lands_below_the_cap():
+    h2 = np.array([1.0, 2.0, 0.5])
+    cnt = np.array([256, 1000, 4096])
+    got = retry_h2(h2, cnt)
+    # uniform medium: the scaled radius holds the target count
+    np.testing.assert_allclose(cnt * (got / h2) ** 1.5, 32.0, rtol=1e-12)
+
+
+def test_fixed_rule_overflows_the_core_and_reevaluates():
+    x, v, m, eps2 = _cluster(1536, seed=7)
+    pol = H.FixedH2()
+    # a radius large enough that the core overflows the 256-entry lists
+    sim = H.BlockHermite6(x, v, m, eps2, pol, backend=OracleBackend(len(m)))
+    sim.h2_fix *= 6.0
+    for _ in range(6):
+        sim.step()
+    st = sim.stats
+    assert st["overflow"] > 0 and st["retries"] >= st["overflow"]
+    # after re-evaluation no particle is left over the cap
+    assert np.all(sim.n_prev < NGB_PB)
+
+
+def test_integrator_conserves_energy_and_radius_does_not_change_forces():
+    x, v, m, eps2 = _cluster(1024, seed=8)
+    out = []
+    for pol in (H.FixedH2(), H.CountScaledH2()):
+        sim = H.BlockHermite6(x, v, m, eps2, pol, backend=OracleBackend(len(m)))
+        for _ in range(25):
+            sim.step()
+        de = abs(sim.energy() - sim.e0) / abs(sim.e0)
+        assert de < 1e-6, de
+        out.append((sim.x.copy(), sim.v.copy(), sim.t.copy(), sim.stats))
+    (x1, v1, t1, s1), (x2, v2, t2, s2) = out
+    assert np.array_equal(t1, t2)
+    assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
+    # the count-scaled rule lands more evaluations in the target range
+    assert s2["in_range"] > s1["in_range"]
+
+
+@pytest.mark.gpu
+def test_learned_radius_cuts_overflow_retries(gpu):
+    x, v, m, eps2 = _cluster(32768, seed=5)
+    runs = {}
+    for name in ("fixed", "learned"):
+        pol = H.FixedH2() if name == "fixed" else (lambda sap: H.LearnedH2(sap, seed=5))
+        sim = H.BlockHermite6(x, v, m, eps2, pol)
+        for _ in range(40):
+            sim.step()
+        runs[name] = (sim.x.copy(), sim.v.copy(), dict(sim.stats))
+        sim.close()
+    (xf, vf, sf), (xl, vl, sl) = runs["fixed"], runs["learned"]
+    # equal step results: forces do not depend on the radius
+    assert np.array_equal(xf, xl) and np.array_equal(vf, vl)
+    assert sf["retries"] >= 5 * max(sl["retries"], 1), (sf, sl)
+    assert sl["in_range"] > sf["in_range"], (sf, sl)
