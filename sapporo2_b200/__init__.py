@@ -34,7 +34,9 @@ F_PREDICT = 1
 F_NGB_LIST = 2
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "lib" / "libsapporo_b200.so"
+# SAPPORO_B200_LIB selects another build of the library (e.g. a variant
+# compiled with different kernel options); default: the in-tree build
+LIB_PATH = Path(os.environ.get("SAPPORO_B200_LIB", _PKG / "lib" / "libsapporo_b200.so"))
 
 _lib = None
 

@@ -127,6 +127,14 @@ __global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti,
 // after the loop.  Rescans recompute ds2 bit-identically (same rounded
 // operations).
 // ========================================================================
+// Unroll depth of the packed j loop (B200, 6th order, N = 2^20: 1 -> 501,
+// 2 -> 526, 4 -> 530 G interactions/s).
+#ifndef SAPB_JUNROLL
+#define SAPB_JUNROLL 4
+#endif
+#define SAPB_STR(x) #x
+#define SAPB_UNROLL(n) _Pragma(SAPB_STR(unroll n))
+
 template <int ORDER, int PREC, int TPI, int IP>
 __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
     force_kernel(ForceArgs A) {
@@ -278,14 +286,17 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           Q[q] = AccMix2{z2, z2, z2, z2, z2, z2, z2, z2, z2, z2};
           tm[q] = make_float2(FLT_MAX, FLT_MAX);
         }
-#pragma unroll 2
-        for (int k = ty; k < cnt; k += TPI) {
-          const float4 r0 = rec[k * C::RS + 0];
-          const float4 r1 = rec[k * C::RS + 1];
-          const float4 r2 = rec[k * C::RS + 2];
-          const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+        {
+          SAPB_UNROLL(SAPB_JUNROLL)
+          for (int k = ty; k < cnt; k += TPI) {
+            const float4 r0 = rec[k * C::RS + 0];
+            const float4 r1 = rec[k * C::RS + 1];
+            const float4 r2 = rec[k * C::RS + 2];
+            const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
 #pragma unroll
-          for (int q = 0; q < NPAIR; q++) pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
+            for (int q = 0; q < NPAIR; q++)
+              pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
+          }
         }
 #pragma unroll
         for (int q = 0; q < NPAIR; q++) {

@@ -181,24 +181,39 @@ __device__ __forceinline__ IMix2 pack_i2(const IMix &a, const IMix &b) {
   return I;
 }
 
-template <int ORDER>
-__device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, const float4 &r1,
-                                          const float4 &r2, const float4 &r3, float2 eps2,
-                                          AccMix2 &A, float2 &tmin) {
+// Two stages: (1) position difference, ds2 and rsqrt on the MUFU pipe,
+// (2) the FMA-pipe bulk.  (Issuing stage 1 of record j+1 before stage 2 of
+// record j by hand measured 6 % slower on B200 than letting the compiler
+// interleave an unrolled loop.)
+struct Pre2 {
+  float2 dx, dy, dz, inv;
+};
+
+__device__ __forceinline__ Pre2 pair_mix2_pre(const IMix2 &I, const float4 &r0, const float4 &r1,
+                                              float2 eps2, float2 &tmin) {
+  Pre2 P;
   // x - y == x + (-y) exactly, so these equal ds_sub of the scalar path
-  float2 dx = __fadd2_rn(__fadd2_rn(bc2(r0.x), I.nxh), __fadd2_rn(bc2(r1.x), I.nxl));
-  const float2 dy = __fadd2_rn(__fadd2_rn(bc2(r0.y), I.nyh), __fadd2_rn(bc2(r1.y), I.nyl));
-  const float2 dz = __fadd2_rn(__fadd2_rn(bc2(r0.z), I.nzh), __fadd2_rn(bc2(r1.z), I.nzl));
+  P.dx = __fadd2_rn(__fadd2_rn(bc2(r0.x), I.nxh), __fadd2_rn(bc2(r1.x), I.nxl));
+  P.dy = __fadd2_rn(__fadd2_rn(bc2(r0.y), I.nyh), __fadd2_rn(bc2(r1.y), I.nyl));
+  P.dz = __fadd2_rn(__fadd2_rn(bc2(r0.z), I.nzh), __fadd2_rn(bc2(r1.z), I.nzl));
   const int idj = __float_as_int(r1.w);
-  dx.x = (idj == I.ida) ? 1.0e18f : dx.x;
-  dx.y = (idj == I.idb) ? 1.0e18f : dx.y;
-  const float2 ds2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+  P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
+  P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
+  const float2 ds2 = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dx, P.dx)));
   tmin.x = fminf(tmin.x, ds2.x);
   tmin.y = fminf(tmin.y, ds2.y);
   const float2 r2v = __fadd2_rn(ds2, eps2);
-  const float2 inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
+  P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
+  return P;
+}
+
+template <int ORDER>
+__device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, float mj,
+                                               const float4 &r2, const float4 &r3,
+                                               AccMix2 &A) {
+  const float2 dx = P.dx, dy = P.dy, dz = P.dz, inv = P.inv;
   const float2 inv2 = __fmul2_rn(inv, inv);
-  const float2 minv = __fmul2_rn(bc2(r0.w), inv);
+  const float2 minv = __fmul2_rn(bc2(mj), inv);
   const float2 minv3 = __fmul2_rn(minv, inv2);
   A.ax = __ffma2_rn(minv3, dx, A.ax);
   A.ay = __ffma2_rn(minv3, dy, A.ay);
@@ -234,6 +249,14 @@ __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, cons
     A.sy = __ffma2_rn(c6, ty, __ffma2_rn(minv3, uy, A.sy));
     A.sz = __ffma2_rn(c6, tz, __ffma2_rn(minv3, uz, A.sz));
   }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, const float4 &r1,
+                                          const float4 &r2, const float4 &r3, float2 eps2,
+                                          AccMix2 &A, float2 &tmin) {
+  const Pre2 P = pair_mix2_pre(I, r0, r1, eps2, tmin);
+  pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
 
 // ---------------- FP64 pair ----------------
