@@ -38,6 +38,12 @@ FLOPS_4TH, FLOPS_6TH = 38, 60
 METRIC = "interactions/s at N=2^20 mixed vs plain FP64, 1 GPU, acc err<=1e-6; %FP32 peak"
 
 
+# DRAM bytes of one mixed 6th-order force launch at N = 2^20, all i, from
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (one pass) of
+# `bench.py --steps 1 --warmup 0 --only mixed --no-cpu`
+FORCE_DRAM_BYTES = 837.37e6 + 117.70e6
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -126,20 +132,32 @@ def measured_peaks() -> dict:
 LAUNCH = None  # (tpi, ip, slices) override for the force kernel, from --launch
 
 
-def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists=False):
+def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists=False,
+               shard=None):
     """Predictor + force on all N with device-resident inputs.  Returns
-    per-step predictor / force times (ms) and the results."""
+    per-step predictor / force (+ combine) times (ms) and the results.
+
+    shard = (rank, world): this rank holds the j with address % world ==
+    rank (the reference's round-robin split over devices) and computes
+    their partial forces on every i; the partials are combined by NCCL
+    all-reduces (sum of forces, min of nearest-neighbour keys) on the same
+    stream, inside the timed step."""
     import sapporo2_b200 as sp
+    from sapporo2_b200.sharded import combine_partials
     n = cfg["n"]
+    rank, world = shard if shard else (0, 1)
+    jsel = np.arange(rank, n, world)
+    nj = len(jsel)
     s = sp.Sapporo(order=sp.SIXTH, precision=precision)
     # a dedicated stream: the library and the timing events must share it
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
     if LAUNCH and precision == sp.DOUBLESINGLE:
         s.set_launch(*LAUNCH)
-    s.set_j_particles(np.arange(n), cfg["id"], cfg["t0"], cfg["m"], cfg["x"], cfg["v"], cfg["a"],
-                      cfg["j"], cfg["s"], cfg["c"])
-    s.force_prediction(n)  # uploads and scatters j (no prediction: no set_time yet)
+    s.set_j_particles(np.arange(nj), cfg["id"][jsel], cfg["t0"][jsel], cfg["m"][jsel],
+                      cfg["x"][jsel], cfg["v"][jsel], cfg["a"][jsel], cfg["j"][jsel],
+                      cfg["s"][jsel], cfg["c"][jsel])
+    s.force_prediction(nj)  # uploads and scatters j (no prediction: no set_time yet)
     rec = sp.pack_i_records(2, cfg["px"], cfg["pv"], cfg["h2"], cfg["id"], cfg["pa"])
     i_dev = torch.from_numpy(rec).cuda()
     res = torch.zeros((n, sp.RES_STRIDE), dtype=torch.float64, device="cuda")
@@ -147,56 +165,68 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
     lst = torch.zeros(n * sp.NGB_PB, dtype=torch.int32, device="cuda") if lists else None
     flags = sp.F_NGB_LIST if lists else 0
     lib, dev = s.lib, s.dev
-    tpi, ip, ns = s.plan(n, n)
-    pred_ms, force_ms = [], []
+    tpi, ip, ns = s.plan(n, nj)
+    pred_ms, force_ms, comb_ms = [], [], []
     torch.cuda.synchronize()
     for it in range(warmup + steps):
         flush()
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
         e0.record(stream)
-        rc = lib.sapb_predict(dev, n, float(cfg["ti"]))
+        rc = lib.sapb_predict(dev, nj, float(cfg["ti"]))
         e1.record(stream)
-        rc |= lib.sapb_force_device(dev, n, n, i_dev.data_ptr(), float(cfg["eps2"]), flags,
+        rc |= lib.sapb_force_device(dev, nj, n, i_dev.data_ptr(), float(cfg["eps2"]), flags,
                                     res.data_ptr(), cnt.data_ptr() if lists else None,
                                     lst.data_ptr() if lists else None)
         e2.record(stream)
         if rc:
             raise RuntimeError(f"device step failed: {lib.sapb_last_error(dev).decode()}")
-        e2.synchronize()
+        if world > 1:
+            with torch.cuda.stream(stream):
+                combine_partials(res)
+        e3.record(stream)
+        e3.synchronize()
         if it >= warmup:
             pred_ms.append(e0.elapsed_time(e1))
             force_ms.append(e1.elapsed_time(e2))
+            comb_ms.append(e2.elapsed_time(e3))
     stream.synchronize()
     out = res.cpu().numpy()
     s.close()
-    return {"pred_ms": pred_ms, "force_ms": force_ms, "res": out,
-            "plan": {"tpi": tpi, "ip": ip, "nslices": ns},
+    return {"pred_ms": pred_ms, "force_ms": force_ms, "comb_ms": comb_ms, "res": out,
+            "plan": {"tpi": tpi, "ip": ip, "nslices": ns}, "nj_local": nj,
             "launches_per_step": 2 + (1 if ns > 1 else 0)}
 
 
-def e2e_arm(cfg, steps: int):
-    """The public class API with host buffers, n_pipes chunks."""
+def e2e_arm(cfg, steps: int, shard=None):
+    """The public class API with host buffers, n_pipes chunks (with shard,
+    the class on each rank behind ShardedSapporo: the rank's j share, NCCL
+    combine of the partial results)."""
     import sapporo2_b200 as sp
     n = cfg["n"]
     s = sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE)
     npipes = s.get_n_pipes()
+    api = s
+    if shard:
+        from sapporo2_b200.sharded import ShardedSapporo
+        api = ShardedSapporo(s, device="cuda")
     times = []
     for it in range(steps + 1):  # first pass warms the pinned buffers
         t0 = time.perf_counter()
-        s.set_j_particles(np.arange(n), cfg["id"], cfg["t0"], cfg["m"], cfg["x"], cfg["v"],
-                          cfg["a"], cfg["j"], cfg["s"], cfg["c"])
-        s.set_time(cfg["ti"])
+        api.set_j_particles(np.arange(n), cfg["id"], cfg["t0"], cfg["m"], cfg["x"], cfg["v"],
+                            cfg["a"], cfg["j"], cfg["s"], cfg["c"])
+        api.set_time(cfg["ti"])
         for i0 in range(0, n, npipes):
             sl = slice(i0, min(n, i0 + npipes))
-            s.start(n, cfg["id"][sl], cfg["px"][sl], cfg["pv"][sl], cfg["pa"][sl], cfg["eps2"],
-                    cfg["h2"][sl])
-            r = s.results(n, ngb=True)
+            api.start(n, cfg["id"][sl], cfg["px"][sl], cfg["pv"][sl], cfg["pa"][sl],
+                      cfg["eps2"], cfg["h2"][sl])
+            r = api.results(n, ngb=True)
         t1 = time.perf_counter()
         if it > 0:
             times.append(t1 - t0)
         del r
     s.close()
-    h2d = n * 22 * 8 + n * 12 * 8
+    world = shard[1] if shard else 1
+    h2d = (n // world) * 22 * 8 + n * 12 * 8
     d2h = n * 12 * 8
     return {"s_per_step": float(np.mean(times)), "h2d": h2d, "d2h": d2h, "chunks": -(-n // npipes)}
 
@@ -432,6 +462,9 @@ def main():
                     default="precision",
                     help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters; "
                          "learned_h2: block steps with fixed, count-scaled and learned h2")
+    ap.add_argument("--multi", choices=["shard", "replicas"], default="shard",
+                    help="N>1 GPUs: shard: one N-body system, j split over the ranks "
+                         "(strong scaling); replicas: an independent system per rank")
     ap.add_argument("--c5-n", type=int, default=262144)
     ap.add_argument("--c5-steps", type=int, default=200)
     ap.add_argument("--launch", default=None,
@@ -469,7 +502,10 @@ def main():
         run_learned_h2_bench(args)
         return
     n = args.n
-    cfg = build_inputs(n, seed=3 + rank)
+    sharded = world > 1 and args.multi == "shard"
+    shard = (rank, world) if sharded else None
+    # j-shards: every rank builds the same system; replicas: one per rank
+    cfg = build_inputs(n, seed=3 if sharded else 3 + rank)
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def flush():
@@ -480,33 +516,39 @@ def main():
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    mix = device_arm(cfg, sp.DOUBLESINGLE, args.steps, args.warmup, torch, flush)
+    mix = device_arm(cfg, sp.DOUBLESINGLE, args.steps, args.warmup, torch, flush, shard=shard)
     clk = clocks.stop()
     torch.cuda.synchronize()
-    step_ms = np.array(mix["pred_ms"]) + np.array(mix["force_ms"])
+    step_ms = np.array(mix["pred_ms"]) + np.array(mix["force_ms"]) + np.array(mix["comb_ms"])
     total_ms = float(step_ms.sum())
     if dist:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     inter_step = float(n) * n
-    value = inter_step * args.steps * world / (total_ms * 1e-3)
+    # replicas: every rank does a whole step; j-shards: the ranks share one
+    jobs = 1 if sharded else world
+    value = inter_step * args.steps * jobs / (total_ms * 1e-3)
 
     if args.only == "mixed":
         print(json.dumps({"metric": METRIC, "value": value, "unit": "interactions/s",
                           "force_ms": float(np.mean(mix["force_ms"])),
                           "pred_ms": float(np.mean(mix["pred_ms"])), "plan": mix["plan"]}))
         return
-    f64 = device_arm(cfg, sp.DOUBLE, args.fp64_steps, 1, torch, flush)
-    f64_ms = np.array(f64["pred_ms"]) + np.array(f64["force_ms"])
-    f64_value = inter_step / (f64_ms.mean() * 1e-3)
+    f64 = device_arm(cfg, sp.DOUBLE, args.fp64_steps, 1, torch, flush, shard=shard)
+    f64_ms = np.array(f64["pred_ms"]) + np.array(f64["force_ms"]) + np.array(f64["comb_ms"])
+    if dist:
+        t = torch.tensor([float(f64_ms.mean())], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        f64_ms = np.array([float(t.item())])
+    f64_value = inter_step / (f64_ms.mean() * 1e-3)  # per job
 
-    e2e = e2e_arm(cfg, args.e2e_steps)
+    e2e = e2e_arm(cfg, args.e2e_steps, shard=shard)
     e2e_value = inter_step / e2e["s_per_step"]
     if dist:
         t = torch.tensor([e2e["s_per_step"]], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = inter_step * world / float(t.item())
+        e2e_value = inter_step * jobs / float(t.item())
 
     if rank != 0:
         if dist:
@@ -520,7 +562,8 @@ def main():
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = nsm * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s
     force_ms = float(np.mean(mix["force_ms"]))
-    achieved = FLOPS_6TH * inter_step / (force_ms * 1e-3) / 1e12
+    nj_loc = mix["nj_local"]  # j this rank's launches stream (all N on one GPU)
+    achieved = FLOPS_6TH * float(n) * nj_loc / (force_ms * 1e-3) / 1e12
     clk_mhz = clk.get("sm_mhz") or sm_max
     fp32_peak_run = nsm * 128 * 2 * clk_mhz * 1e6 / 1e12
     hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -531,28 +574,39 @@ def main():
     result = {
         "metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if sharded else "weak",
+        "vs_baseline": None,
         "dtype": "f32 body + ds positions + f64 sums", "data": "synthetic",
         "config": {"workload": "precision form: Plummer N=2^20, Salpeter masses 0.1-100, 10% "
                                "circular binaries a~logU(1e-6,1e-4), Hermite 6th order, all i "
                                "active, NN on, lists off",
                    "n": n, "order": 6, "precision": "mixed (DS dr, FP32 body, FP64 sums)",
                    "eps2": cfg["eps2"], "l2": "flushed between steps (256 MB write)",
-                   "launch_plan": mix["plan"], "parallelism": f"replicas x{world}"},
+                   "launch_plan": mix["plan"],
+                   "parallelism": (f"j-shards x{world} (round-robin j, NCCL all-reduce of "
+                                   "partial forces and nearest-neighbour keys)") if sharded
+                   else f"replicas x{world}",
+                   "combine_ms": float(np.mean(mix["comb_ms"])), "nj_per_rank": mix["nj_local"]},
         "gflops": value * FLOPS_6TH / 1e9,
-        "fp64": {"value": f64_value * world, "unit": "interactions/s",
-                 "ms_per_step": float(f64_ms.mean()), "speedup_mixed_over_fp64": value / world / f64_value},
+        "fp64": {"value": f64_value * jobs, "unit": "interactions/s",
+                 "ms_per_step": float(f64_ms.mean()),
+                 "speedup_mixed_over_fp64": value / jobs / f64_value},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak, "traffic": None,
+                     "frac": achieved / fp32_peak,
+                     "traffic": FORCE_DRAM_BYTES if (n == 1 << 20 and nj_loc == n) else None,
+                     "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                     "force_kernel<6th,DS> launch at N=2^20 (ncu, 1 pass): "
+                                     "837.4 MB read + 117.7 MB written in 2.07 s, 0.46 GB/s; "
+                                     "j records stream from L2",
                      "peak_note": f"derived: {nsm} SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz "
                                   "(sm_max_mhz of measured peaks; no FP32 entry there)",
                      "frac_at_run_clock": achieved / fp32_peak_run,
                      "flops_per_interaction": FLOPS_6TH, "kernel": "force_kernel<6th,DS>",
                      "force_ms": force_ms},
         "roofline_predictor": {"bound": "hbm",
-                               "achieved": pred_bytes * n / (pred_ms * 1e-3) / 1e9,
+                               "achieved": pred_bytes * nj_loc / (pred_ms * 1e-3) / 1e9,
                                "peak": hbm, "unit": "GB/s",
-                               "frac": pred_bytes * n / (pred_ms * 1e-3) / 1e9 / hbm,
+                               "frac": pred_bytes * nj_loc / (pred_ms * 1e-3) / 1e9 / hbm,
                                "bytes_per_j": pred_bytes, "bytes_moved_per_j": pred_read_write,
                                "pred_ms": pred_ms, "peak_note": "hbm_gbs of measured peaks"},
         "e2e": {"value": e2e_value, "unit": "interactions/s",

@@ -312,6 +312,29 @@ class Sapporo:
         _check(self.lib.sapb_ngb_fetch(self.dev, cnt, None, ni), "ngb_fetch", self.dev)
         return cnt[:ni]
 
+    def raw_results(self, ni=None) -> np.ndarray:
+        """Result records of the last force call as the device wrote them:
+        [ni, RES_STRIDE] doubles = acc[3], pot, jerk[3], snap[3], ds2 of the
+        nearest neighbour (float value; 1e11 when none), its id (-1 when
+        none).  The input of the multi-GPU combine (sum, min-loc)."""
+        ni = self._ni if ni is None else ni
+        p, n = C.c_void_p(), C.c_int()
+        _check(self.lib.sapb_results(self.dev, C.byref(p), C.byref(n)), "results", self.dev)
+        if n.value < ni:
+            raise SapporoError(f"results hold {n.value} records, {ni} requested")
+        buf = (C.c_double * (ni * RES_STRIDE)).from_address(p.value)
+        return np.frombuffer(buf, dtype=np.float64).reshape(ni, RES_STRIDE).copy()
+
+    def neighbour_lists(self, ni=None):
+        """Counts [ni] and lists [ni, NGB_PB] of the last force call (entries
+        past min(count, NGB_PB) are undefined)."""
+        ni = self._ni if ni is None else ni
+        cnt = np.zeros(max(ni, 1), dtype=np.int32)
+        lst = np.zeros(max(ni, 1) * NGB_PB, dtype=np.int32)
+        self.results_ready()
+        _check(self.lib.sapb_ngb_fetch(self.dev, cnt, lst, ni), "ngb_fetch", self.dev)
+        return cnt[:ni], lst.reshape(-1, NGB_PB)[:ni]
+
     def results_ready(self):
         p, n = C.c_void_p(), C.c_int()
         _check(self.lib.sapb_results(self.dev, C.byref(p), C.byref(n)), "results", self.dev)

@@ -7,7 +7,7 @@ from oracle import oracle as O
 
 
 class OracleBackend:
-    def __init__(self, n):
+    def __init__(self, n, lists=False):
         z = np.zeros((n, 3))
         self.n = n
         self.t = np.zeros(n)
@@ -16,6 +16,7 @@ class OracleBackend:
         self.x, self.v, self.a, self.j, self.s, self.c = (z.copy() for _ in range(6))
         self.ti = 0.0
         self.calls = 0
+        self.lists = lists
 
     def set_j_particles(self, address, id, t, mass, x, v, a, jrk, snp=None, crk=None, eps=None):
         address = np.asarray(address)
@@ -33,7 +34,7 @@ class OracleBackend:
         ni = len(id)
         self._r = O.force(2, xi, vi, ai if ai is not None else np.zeros((ni, 3)),
                           np.zeros(ni) if h2 is None else h2, id, px, pv, pa, self.m[:nj],
-                          self.id[:nj], eps2, lists=False)
+                          self.id[:nj], eps2, lists=self.lists)
         self.calls += 1
 
     def results(self, nj, ni=None, ngb=True):
@@ -41,6 +42,21 @@ class OracleBackend:
 
     def neighbour_counts(self, ni=None):
         return self._r["ngb_count"].copy()
+
+    def raw_results(self, ni=None):
+        """Records in the device layout: acc, pot, jerk, snap, ds2 of the
+        nearest neighbour rounded to float (1e11 when none), its id."""
+        r = self._r
+        n = len(r["pot"])
+        out = np.zeros((n, 12))
+        out[:, 0:3], out[:, 3], out[:, 4:7], out[:, 7:10] = r["acc"], r["pot"], r["jrk"], r["snp"]
+        none = r["nnb"] < 0
+        out[:, 10] = np.where(none, 1.0e11, r["ds2min"].astype(np.float32).astype(np.float64))
+        out[:, 11] = np.where(none, -1, r["nnb"])
+        return out
+
+    def neighbour_lists(self, ni=None):
+        return self._r["ngb_count"].copy(), self._r["ngb_list"].copy()
 
     def close(self):
         pass
