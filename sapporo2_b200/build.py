@@ -100,6 +100,9 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     if relinked or not lib6.exists():
         _run([HOST_CXX, "-shared", "-o", str(lib6), str(obj6), f"-L{LIBDIR}", "-lsapporo_b200",
               "-Wl,-rpath,$ORIGIN"])
+    src_c, bin_c = CSRC / "fma_ceiling.cu", LIBDIR / "fma_ceiling"
+    if force or _stale(bin_c, src_c, []):
+        _run([NVCC, *ARCH, "-O3", "-std=c++17", "-ccbin", HOST_CXX, "-o", str(bin_c), str(src_c)])
     if verbose:
         print(f"built {lib}")
     return lib

@@ -286,17 +286,15 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           Q[q] = AccMix2{z2, z2, z2, z2, z2, z2, z2, z2, z2, z2};
           tm[q] = make_float2(FLT_MAX, FLT_MAX);
         }
-        {
-          SAPB_UNROLL(SAPB_JUNROLL)
-          for (int k = ty; k < cnt; k += TPI) {
-            const float4 r0 = rec[k * C::RS + 0];
-            const float4 r1 = rec[k * C::RS + 1];
-            const float4 r2 = rec[k * C::RS + 2];
-            const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+        SAPB_UNROLL(SAPB_JUNROLL)
+        for (int k = ty; k < cnt; k += TPI) {
+          const float4 r0 = rec[k * C::RS + 0];
+          const float4 r1 = rec[k * C::RS + 1];
+          const float4 r2 = rec[k * C::RS + 2];
+          const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
 #pragma unroll
-            for (int q = 0; q < NPAIR; q++)
-              pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
-          }
+          for (int q = 0; q < NPAIR; q++)
+            pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
         }
 #pragma unroll
         for (int q = 0; q < NPAIR; q++) {

@@ -67,9 +67,12 @@ class LearnedH2:
 
     name = "learned"
 
-    def __init__(self, sap, seed=5, epochs=8, lr=2e-3, pre_epochs=300):
+    def __init__(self, sap, seed=5, epochs=4, lr=1e-3, pre_epochs=300, max_batch=8192,
+                 max_pre=65536):
         self.net = H2Net(sap, seed=seed)
         self.epochs, self.lr, self.pre_epochs = epochs, lr, pre_epochs
+        self.max_batch, self.max_pre = max_batch, max_pre
+        self.rng = np.random.default_rng(seed)
         self.losses = []
         self.train_s = 0.0
         self.pretrain_s = 0.0
@@ -78,6 +81,9 @@ class LearnedH2:
         t0 = time.perf_counter()
         f = np.concatenate([s[0] for s in samples])
         y = np.concatenate([s[1] - self.net.base_log_ratio(s[2]) for s in samples])
+        if len(f) > self.max_pre:
+            take = self.rng.choice(len(f), self.max_pre, replace=False)
+            f, y = f[take], y[take]
         self.net.fit_standardisation(f)
         for _ in range(self.pre_epochs // 50):
             self.losses.append(self.net.train(self.net.standardise(f), y, 50, 3e-3))
@@ -87,9 +93,15 @@ class LearnedH2:
         return self.net.propose(sim.n_prev[idx], sim.h2_prev[idx], sim.a[idx], sim.j[idx])
 
     def observe(self, sim, idx, h2_used, counts):
+        """One online update on (at most max_batch of) this step's first
+        attempts."""
         t0 = time.perf_counter()
-        loss = self.net.learn(sim.n_prev[idx], sim.h2_prev[idx], sim.a[idx], sim.j[idx], h2_used,
-                              counts, epochs=self.epochs, lr=self.lr)
+        take = np.arange(len(idx))
+        if len(take) > self.max_batch:
+            take = self.rng.choice(len(idx), self.max_batch, replace=False)
+        q = idx[take]
+        loss = self.net.learn(sim.n_prev[q], sim.h2_prev[q], sim.a[q], sim.j[q], h2_used[take],
+                              counts[take], epochs=self.epochs, lr=self.lr)
         self.losses.append(loss)
         self.train_s += time.perf_counter() - t0
 

@@ -127,16 +127,27 @@ class H2Net:
         (target / previous count)^(2/3)."""
         return (2.0 / 3.0) * np.log(target / np.maximum(np.asarray(n_prev, dtype=np.float64), 0.5))
 
+    # The correction may shrink h2 by up to e^MAX_DOWN but grow it by at most
+    # e^MAX_UP (x1.45 in the expected count): an overflow costs a whole
+    # re-evaluation of the particle, a list below the target range costs
+    # nothing, so the network is not allowed to gamble on growing a radius.
+    MAX_DOWN = 1.0
+    MAX_UP = 0.25
+
     def propose(self, n_prev, h2_prev, acc, jrk, clip=4.0) -> np.ndarray:
         """h2 for the next evaluation: the count-scaled radius times the
-        network's correction (log-ratio clipped to +-clip)."""
+        network's bounded correction; the whole log-ratio is clipped to
+        +-clip."""
         f = self.standardise(features(n_prev, h2_prev, acc, jrk))
-        r = self.base_log_ratio(n_prev) + self.forward(f).astype(np.float64)
+        corr = np.clip(self.forward(f).astype(np.float64), -self.MAX_DOWN, self.MAX_UP)
+        r = self.base_log_ratio(n_prev) + corr
         return np.asarray(h2_prev) * np.exp(np.clip(r, -clip, clip))
 
     def learn(self, n_prev, h2_prev, acc, jrk, h2_used, n_obs, epochs=20, lr=2e-3) -> float:
         """One online update: the correction that would have given the target
-        count, from the count the force kernel found with h2_used."""
+        count, from the count the force kernel found with h2_used (clipped to
+        the correction's bounds, so a particle that found no neighbour does
+        not drag the fit)."""
         f = self.standardise(features(n_prev, h2_prev, acc, jrk))
         y = target_log_ratio(h2_used, h2_prev, n_obs) - self.base_log_ratio(n_prev)
-        return self.train(f, y, epochs, lr)
+        return self.train(f, np.clip(y, -self.MAX_DOWN, self.MAX_UP), epochs, lr)

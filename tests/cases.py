@@ -20,12 +20,14 @@ H2_BAND = 1e-6
 
 def build_case(order: int, n: int, seed: int, eps2: float = 1e-6, binaries: float = 0.0,
                salpeter: bool = False, nngb: float = 32.0, id_offset: int = 100,
-               t_spread: bool = True) -> dict:
+               t_spread: bool = True, permute_ids: bool = False) -> dict:
     m = ic.salpeter(n, seed) if salpeter else None
     x, v, m = ic.plummer(n, seed, masses=m)
     if binaries > 0:
         x, v, m, _ = ic.add_binaries(x, v, m, binaries, seed + 11)
     ids = (np.arange(n) + id_offset).astype(np.int32)
+    if permute_ids:  # ids unrelated to the addresses: every j tile spans all ids
+        ids = ids[np.random.default_rng(seed + 7).permutation(n)]
     fn = O.derivative_fn()
     a, j, _ = fn(1, x, v, None, m, ids, eps2)
     s = c = None

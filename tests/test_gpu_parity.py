@@ -50,6 +50,22 @@ def test_launch_shapes_agree(gpu, order, precision, launch):
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want, sel=sel)
 
 
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("permute", [False, True])
+@pytest.mark.parametrize("launch", [(1, 4, 0), (1, 2, 0), (2, 2, 3)])
+def test_self_pair_both_tile_paths(gpu, order, permute, launch):
+    """Tiles whose ids cannot contain a warp's i skip the self-pair compare;
+    ids in address order (mostly skipped) and permuted ids (never skipped)
+    give the oracle's answer, with the self pair excluded either way."""
+    case = T.build_case(order, 1500, seed=15, binaries=0.1, permute_ids=permute)
+    want = T.oracle_force(case)
+    got = T.run_library(case, sp.DOUBLESINGLE, launch=launch)
+    T.check_forces(got, want, order)
+    T.check_nn(case, got["nnb"], want)
+    assert not np.any(got["nnb"] == case["id"])
+    T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want)
+
+
 @pytest.mark.parametrize("ni", [1, 2, 31, 127, 129, 255, 257])
 def test_small_active_sets(gpu, ni):
     case = T.build_case(2, 3000, seed=14)
