@@ -127,28 +127,27 @@ __device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const 
   const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
   const float m3i2 = -3.0f * inv2;
   if (ORDER == FOURTH) {
-    // jerk += m/r^3 dv - 3 m/r^5 (dr.dv) dr   (kernels.cu:631-637)
-    const float c = (m3i2 * minv3) * rv;
-    A.jx = fmaf(c, dx, fmaf(minv3, dvx, A.jx));
-    A.jy = fmaf(c, dy, fmaf(minv3, dvy, A.jy));
-    A.jz = fmaf(c, dz, fmaf(minv3, dvz, A.jz));
+    // jerk += m/r^3 (dv - 3 (dr.dv)/r^2 dr)   (kernels.cu:631-637)
+    const float a3 = m3i2 * rv;
+    A.jx = fmaf(minv3, fmaf(a3, dx, dvx), A.jx);
+    A.jy = fmaf(minv3, fmaf(a3, dy, dvy), A.jy);
+    A.jz = fmaf(minv3, fmaf(a3, dz, dvz), A.jz);
   } else {
     // kernels.cu:642-667 with a3 = -3 alpha, b3 = -3 beta:
     //   jerk_ij = minv3 (dv + a3 dr)
-    //   snap   += minv3 (da + b3 dr) + 2 a3 jerk_ij
+    //   snap   += minv3 (da + b3 dr) + 2 a3 jerk_ij = minv3 (da + b3 dr + 2 a3 t)
     const float dax = r3.x - I.ax, day = r3.y - I.ay, daz = r3.z - I.az;
     const float s = fmaf(dz, daz, fmaf(dy, day, fmaf(dx, dax, fmaf(dvz, dvz, fmaf(dvy, dvy, dvx * dvx)))));
     const float a3 = m3i2 * rv;
     const float b3 = fmaf(a3, a3 * (-1.0f / 3.0f), s * m3i2);
-    const float c6 = (a3 + a3) * minv3;
+    const float a6 = a3 + a3;
     const float tx = fmaf(a3, dx, dvx), ty = fmaf(a3, dy, dvy), tz = fmaf(a3, dz, dvz);
     A.jx = fmaf(minv3, tx, A.jx);
     A.jy = fmaf(minv3, ty, A.jy);
     A.jz = fmaf(minv3, tz, A.jz);
-    const float ux = fmaf(b3, dx, dax), uy = fmaf(b3, dy, day), uz = fmaf(b3, dz, daz);
-    A.sx = fmaf(c6, tx, fmaf(minv3, ux, A.sx));
-    A.sy = fmaf(c6, ty, fmaf(minv3, uy, A.sy));
-    A.sz = fmaf(c6, tz, fmaf(minv3, uz, A.sz));
+    A.sx = fmaf(minv3, fmaf(a6, tx, fmaf(b3, dx, dax)), A.sx);
+    A.sy = fmaf(minv3, fmaf(a6, ty, fmaf(b3, dy, day)), A.sy);
+    A.sz = fmaf(minv3, fmaf(a6, tz, fmaf(b3, dz, daz)), A.sz);
   }
 }
 
@@ -232,10 +231,10 @@ __device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, fl
   const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
   const float2 m3i2 = __fmul2_rn(bc2(-3.0f), inv2);
   if (ORDER == FOURTH) {
-    const float2 c = __fmul2_rn(__fmul2_rn(m3i2, minv3), rv);
-    A.jx = __ffma2_rn(c, dx, __ffma2_rn(minv3, dvx, A.jx));
-    A.jy = __ffma2_rn(c, dy, __ffma2_rn(minv3, dvy, A.jy));
-    A.jz = __ffma2_rn(c, dz, __ffma2_rn(minv3, dvz, A.jz));
+    const float2 a3 = __fmul2_rn(m3i2, rv);
+    A.jx = __ffma2_rn(minv3, __ffma2_rn(a3, dx, dvx), A.jx);
+    A.jy = __ffma2_rn(minv3, __ffma2_rn(a3, dy, dvy), A.jy);
+    A.jz = __ffma2_rn(minv3, __ffma2_rn(a3, dz, dvz), A.jz);
   } else {
     const float2 dax = __fadd2_rn(bc2(r3.x), I.nax);
     const float2 day = __fadd2_rn(bc2(r3.y), I.nay);
@@ -244,17 +243,15 @@ __device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, fl
                      __ffma2_rn(dvz, dvz, __ffma2_rn(dvy, dvy, __fmul2_rn(dvx, dvx))))));
     const float2 a3 = __fmul2_rn(m3i2, rv);
     const float2 b3 = __ffma2_rn(a3, __fmul2_rn(a3, bc2(-1.0f / 3.0f)), __fmul2_rn(s, m3i2));
-    const float2 c6 = __fmul2_rn(__fadd2_rn(a3, a3), minv3);
+    const float2 a6 = __fadd2_rn(a3, a3);
     const float2 tx = __ffma2_rn(a3, dx, dvx), ty = __ffma2_rn(a3, dy, dvy),
                  tz = __ffma2_rn(a3, dz, dvz);
     A.jx = __ffma2_rn(minv3, tx, A.jx);
     A.jy = __ffma2_rn(minv3, ty, A.jy);
     A.jz = __ffma2_rn(minv3, tz, A.jz);
-    const float2 ux = __ffma2_rn(b3, dx, dax), uy = __ffma2_rn(b3, dy, day),
-                 uz = __ffma2_rn(b3, dz, daz);
-    A.sx = __ffma2_rn(c6, tx, __ffma2_rn(minv3, ux, A.sx));
-    A.sy = __ffma2_rn(c6, ty, __ffma2_rn(minv3, uy, A.sy));
-    A.sz = __ffma2_rn(c6, tz, __ffma2_rn(minv3, uz, A.sz));
+    A.sx = __ffma2_rn(minv3, __ffma2_rn(a6, tx, __ffma2_rn(b3, dx, dax)), A.sx);
+    A.sy = __ffma2_rn(minv3, __ffma2_rn(a6, ty, __ffma2_rn(b3, dy, day)), A.sy);
+    A.sz = __ffma2_rn(minv3, __ffma2_rn(a6, tz, __ffma2_rn(b3, dz, daz)), A.sz);
   }
 }
 
