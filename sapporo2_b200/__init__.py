@@ -137,6 +137,24 @@ _SIGS = [
     ("sapporo_c_last_status", C.c_int, [C.c_void_p]),
     ("sapporo_c_device", C.c_void_p, [C.c_void_p]),
     # GRAPE-6
+    # GRAPE-5 interface
+    ("g5_open_special", C.c_int, [C.c_int, C.POINTER(C.c_int)]),
+    ("g5_open", None, []),
+    ("g5_close", None, []),
+    ("g5_get_number_of_pipelines", C.c_int, []),
+    ("g5_set_n", None, [C.c_int]),
+    ("g5_set_eps2_to_all", None, [C.c_double]),
+    ("g5_set_eps_to_all", None, [C.c_double]),
+    ("g5_set_xmj", None, [C.c_int, C.c_int, _dp, _dp]),
+    ("g5_set_jp", None, [C.c_int, C.c_int, _dp, _dp]),
+    ("g5_set_xi", None, [C.c_int, _dp]),
+    ("g5_run", None, []),
+    ("g5_get_force", None, [C.c_int, _dp, _dp]),
+    ("g5_calculate_force_on_x", None, [_dp, _dp, _dp, C.c_int]),
+    ("g5_set_range", None, [C.c_double, C.c_double, C.c_double]),
+    ("g5_get_jmemsize", C.c_int, []),
+    ("g5_get_number_of_real_pipelines", C.c_int, []),
+    ("g5_get_pcibus_freq", C.c_int, []),
     ("g6_open_", C.c_int, [C.POINTER(C.c_int)]),
     ("g6_open_special", C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     ("g6_close_", C.c_int, [C.POINTER(C.c_int)]),
@@ -373,6 +391,42 @@ class Sapporo:
     def set_stream(self, stream_ptr: int | None):
         _check(self.lib.sapb_set_stream(self.dev, C.c_void_p(stream_ptr or 0)), "set_stream",
                self.dev)
+
+
+class G5:
+    """The GRAPE-5 interface (positions and masses in, acceleration and
+    potential out), through its C ABI; one process-wide instance."""
+
+    def __init__(self, devices=(0,)):
+        self.lib = load_library()
+        arr = (C.c_int * len(devices))(*devices)
+        _check(self.lib.g5_open_special(len(devices), arr), "g5_open_special")
+
+    def close(self):
+        self.lib.g5_close()
+
+    def set_eps(self, eps):
+        self.lib.g5_set_eps_to_all(float(eps))
+
+    def set_j(self, x, m):
+        x, m = _f64(x), _f64(m)
+        self.lib.g5_set_n(len(m))
+        self.lib.g5_set_xmj(0, len(m), x, m)
+
+    def force(self, xi):
+        xi = _f64(xi)
+        a, phi = np.zeros((len(xi), 3)), np.zeros(len(xi))
+        self.lib.g5_calculate_force_on_x(xi, a, phi, len(xi))
+        return a, phi
+
+    def force_chunk(self, xi):
+        """g5_set_xi + g5_get_force (ni <= n_pipes)."""
+        xi = _f64(xi)
+        a, phi = np.zeros((len(xi), 3)), np.zeros(len(xi))
+        self.lib.g5_set_xi(len(xi), xi)
+        self.lib.g5_run()
+        self.lib.g5_get_force(len(xi), a, phi)
+        return a, phi
 
 
 class G6:

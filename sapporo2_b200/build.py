@@ -24,6 +24,7 @@ BUILD = PKG / "_build"
 LIBDIR = PKG / "lib"
 LIBNAME = "libsapporo_b200.so"
 LIB6TH = "libsapporo6th_b200.so"  # 6th-order C interface (generic names, own library)
+LIBYEB = "libsapporoyeb_b200.so"  # the Yebisu 6th-order interface (same generic names)
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
@@ -40,7 +41,7 @@ CXX_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra", f"-I{INCLUDE}", f
 
 CU_SOURCES = ["sapb_kernels.cu", "sapb_capi.cu", "sapb_batch_kernels.cu", "sapb_batch.cu",
               "sapb_mlp.cu"]
-CXX_SOURCES = ["sapporohostclass.cpp", "sapporoG6lib.cpp", "sapporo_cbind.cpp"]
+CXX_SOURCES = ["sapporohostclass.cpp", "sapporoG6lib.cpp", "sapporoG5lib.cpp", "sapporo_cbind.cpp"]
 
 
 def _headers() -> list[Path]:
@@ -99,7 +100,15 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         relinked = True
     if relinked or not lib6.exists():
         _run([HOST_CXX, "-shared", "-o", str(lib6), str(obj6), f"-L{LIBDIR}", "-lsapporo_b200",
-              "-Wl,-rpath,$ORIGIN"])
+              "-Wl,-rpath,$ORIGIN", "-Wl,-Bsymbolic"])
+    srcy, objy, liby = CSRC / "sapporoYeblib.cpp", BUILD / "sapporoYeblib.cpp.o", LIBDIR / LIBYEB
+    rely = relinked
+    if force or _stale(objy, srcy, deps):
+        _run([HOST_CXX, *CXX_FLAGS, "-c", str(srcy), "-o", str(objy)])
+        rely = True
+    if rely or not liby.exists():
+        _run([HOST_CXX, "-shared", "-o", str(liby), str(objy), f"-L{LIBDIR}", "-lsapporo_b200",
+              "-Wl,-rpath,$ORIGIN", "-Wl,-Bsymbolic"])
     src_c, bin_c = CSRC / "fma_ceiling.cu", LIBDIR / "fma_ceiling"
     if force or _stale(bin_c, src_c, []):
         _run([NVCC, *ARCH, "-O3", "-std=c++17", "-ccbin", HOST_CXX, "-o", str(bin_c), str(src_c)])

@@ -11,14 +11,16 @@ import pytest
 import sapporo2_b200 as sp
 
 INCLUDE = Path(__file__).resolve().parents[1] / "include"
-C_HEADERS = ["sapporo_b200.h", "sapporo_c.h", "sapporo_g6.h"]
+C_HEADERS = ["sapporo_b200.h", "sapporo_c.h", "sapporo_g6.h", "sapporo_g5.h"]
+# interfaces with generic names live in libraries of their own
+OWN_LIBS = {"sapporo6th.h": "libsapporo6th_b200.so", "sapporo_yebisu.h": "libsapporoyeb_b200.so"}
 DECL = re.compile(r"^\s*(?:const\s+)?(?:struct\s+)?[A-Za-z_][\w]*\s*\**\s*\**\s*([a-z_][\w]*)\s*\(",
                   re.M)
 
 
-def declared_c_functions():
+def declared_c_functions(headers=C_HEADERS):
     names = []
-    for h in C_HEADERS:
+    for h in headers:
         text = (INCLUDE / h).read_text()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         text = re.sub(r"#.*", "", text)
@@ -35,6 +37,15 @@ def test_declared_c_symbols_exported():
     names = declared_c_functions()
     assert len(names) >= 40, names
     lib = ctypes.CDLL(str(sp.LIB_PATH))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize("header", sorted(OWN_LIBS))
+def test_interface_libraries_export_their_headers(header):
+    names = declared_c_functions([header])
+    assert len(names) >= 6, names
+    lib = ctypes.CDLL(str(sp.LIB_PATH.parent / OWN_LIBS[header]))
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
 
