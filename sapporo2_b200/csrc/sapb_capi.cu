@@ -189,6 +189,14 @@ static int blocks_per_sm(int order, int prec, int ip) {
   return ip >= 4 ? 2 : 4;  // mixed: <= 128 registers (ip 1, 2), <= 255 (ip 4)
 }
 
+// Launch shape for ni i-particles and nj j: threads-per-i, i per thread and
+// the number of j-slices S.  Cost model: blocks of one shape run in waves
+// of R = SMs x resident blocks per SM; a block of st tiles costs
+// (st + 1) tile-times (prologue, nearest-neighbour rescan, epilogue), a
+// tile-time being 128 x (i per block) x (blocks per SM) pair-times of one
+// SM; S > 1 adds the slice reduction (S x ni records read).  The block
+// count B = i-tiles x S is chosen near a whole number of waves: a last wave
+// that holds a few blocks costs as much as a full one.
 static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   const int tj = force_tile_j();
   const int ntiles = std::max(1, (nj + tj - 1) / tj);
@@ -196,29 +204,47 @@ static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   static const int shapes_mix[][2] = {{1, 4}, {2, 4}, {1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
   static const int shapes_dp[][2] = {{1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
   const int nshape = d->prec == DOUBLE ? 6 : 8;
+  // pair-times per SM and second (B200, measured order of magnitude): only
+  // the balance between force and reduction depends on them
+  const double sm_rate = d->prec == DOUBLE ? (d->order >= SIXTH ? 1.5e9 : 2.3e9)
+                                           : (d->order >= SIXTH ? 3.6e9 : 5.6e9);
+  const int max_ns = std::max(1, ntiles / 4);  // keep >= 4 tiles per slice
   Plan best{1, 2, 1, 1, ntiles};
-  double best_score = -1.0;
+  double best_t = 1e300;
   for (int q = 0; q < nshape; q++) {
     const int *sh = d->prec == DOUBLE ? shapes_dp[q] : shapes_mix[q];
     const int tpi = d->tpi ? d->tpi : sh[0];
     const int ip = d->ip ? d->ip : sh[1];
     const int ti = force_tile_i(tpi, ip);
     const int i_tiles = (ni + ti - 1) / ti;
-    const long target = 2L * d->num_sms * blocks_per_sm(d->order, d->prec, ip);
-    int ns = d->nslices;
-    if (!ns) {
-      const int max_ns = std::max(1, ntiles / 4);  // keep >= 4 tiles per slice
-      ns = (int)std::min<long>(max_ns, (target + i_tiles - 1) / i_tiles);
-      ns = std::max(ns, 1);
-    }
-    const int st = (ntiles + ns - 1) / ns;
-    ns = (ntiles + st - 1) / st;  // every slice non-empty
-    const double fill = std::min(1.0, (double)i_tiles * ns / (double)target);
-    const double used = (double)ni / ((double)i_tiles * ti);
-    const double score = fill * used;
-    if (score > best_score + 1e-9) {
-      best_score = score;
-      best = Plan{tpi, ip, ns, i_tiles, st};
+    const int bps = blocks_per_sm(d->order, d->prec, ip);
+    const long R = (long)d->num_sms * bps;
+    const double speed = ip >= 4 ? 1.0 : (ip == 2 ? 0.97 : 0.8);
+    const double tile_time = 128.0 * ti * bps / (speed * sm_rate);
+    auto consider = [&](int ns) {
+      ns = std::max(1, std::min(ns, max_ns));
+      const int st = (ntiles + ns - 1) / ns;
+      const int nse = (ntiles + st - 1) / st;  // every slice non-empty
+      const long B = (long)i_tiles * nse;
+      const long waves = (B + R - 1) / R;
+      double t = (double)waves * (st + 1.0) * tile_time;
+      if (nse > 1) t += 5e-6 + (double)nse * ni * kResStride * 8.0 / 4.0e12;
+      if (t < best_t * (1.0 - 1e-9)) {
+        best_t = t;
+        best = Plan{tpi, ip, nse, i_tiles, st};
+      }
+    };
+    if (d->nslices) {
+      consider(d->nslices);
+    } else {
+      consider(1);
+      consider(max_ns);
+      for (int k = 1; k <= 64; k++) {  // B just below k whole waves
+        const long ns = (long)k * R / std::max(i_tiles, 1);
+        if (ns < 1) continue;
+        if (ns > max_ns) break;
+        consider((int)ns);
+      }
     }
     if (d->tpi) break;  // fixed shape
   }
