@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <climits>
 #include <new>
 
 #include "../../include/sapporo_b200.h"
@@ -82,6 +83,11 @@ static void bind_planes(JState &js, double *pool, int *id, int cap, int order) {
 // plane and of the predicted records.
 static int grow_j(sapb_dev *d, int new_cap) {
   if (new_cap <= d->cap) return SAPB_OK;
+  // grow the device store by at least half: callers that stage addresses in
+  // order step their bound up by 10 % at a time (the reference's
+  // increase_jMemory), which would otherwise reallocate and copy the whole
+  // store ~44 times on the way from 16384 to 2^20
+  if (d->cap > 0) new_cap = (int)std::min<long long>(INT_MAX / 2, std::max<long long>(new_cap, (long long)d->cap + d->cap / 2));
   const int np = nplanes(d->order);
   double *pool = nullptr;
   int *id = nullptr;
