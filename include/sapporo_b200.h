@@ -120,6 +120,14 @@ int sapb_ngb_fetch(sapb_dev *d, int *counts, int *lists, int ni);
 int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
                       double *res_dev, int *ngb_count_dev, int *ngb_list_dev);
 
+/* Self-test of the device-side failure path (no reference counterpart; the
+ * reference has no bounded waits).  Launches one thread that waits on a
+ * shared-memory barrier nothing ever arrives at, with the same bounded wait
+ * the force kernels use but a limit of limit_ms (1..2000).  Returns
+ * SAPB_ETIMEOUT when the wait gave up and the kernel returned -- the
+ * expected outcome, after which the device stays usable. */
+int sapb_wait_selftest(sapb_dev *d, int limit_ms);
+
 /* Force call that allocates nothing: no cudaMalloc, cudaFree or other
  * allocating routine, on any call.  It is for callers that cannot allocate
  * device memory while they integrate -- codes that hand the whole GPU to

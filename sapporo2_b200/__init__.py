@@ -84,6 +84,7 @@ _SIGS = [
     ("sapb_force", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
     ("sapb_results", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
     ("sapb_ngb_fetch", C.c_int, [C.c_void_p, _ipo, _ipo, C.c_int]),
+    ("sapb_wait_selftest", C.c_int, [C.c_void_p, C.c_int]),
     ("sapb_force_device", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double,
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sapb_force_device_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p,

@@ -593,6 +593,22 @@ int sapb_force_device(sapb_dev *d, int nj, int ni, const double *i_dev, double e
   return run_force(d, nj, ni, i_dev, eps2, flags, res_dev, ngb_count_dev, ngb_list_dev);
 }
 
+int sapb_wait_selftest(sapb_dev *d, int limit_ms) {
+  if (!d || limit_ms < 1 || limit_ms > 2000)
+    return fail(d, SAPB_EINVAL, "wait self-test limit %d ms (1..2000)", limit_ms);
+  CK(d, cudaSetDevice(d->device));
+  CK(d, cudaMemsetAsync(d->status_d, 0, sizeof(int), d->stream));
+  CK(d, launch_wait_selftest((uint64_t)limit_ms * 1000000ull, d->status_d, d->stream));
+  int s = 0;
+  CK(d, cudaMemcpyAsync(&s, d->status_d, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+  CK(d, cudaStreamSynchronize(d->stream));
+  CK(d, cudaMemsetAsync(d->status_d, 0, sizeof(int), d->stream));
+  if (s & kErrWaitTimeout)
+    return fail(d, SAPB_ETIMEOUT, "self-test: the bounded device wait gave up after %d ms",
+                limit_ms);
+  return fail(d, SAPB_ECUDA, "self-test: the wait on a barrier nothing arrives at returned");
+}
+
 int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2,
                               int flags, double *res_dev, int *ngb_count_dev,
                               int *ngb_list_dev) {

@@ -444,6 +444,26 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 }
 
 // ========================================================================
+// Self-test of the bounded device wait: one thread waits on an mbarrier
+// that nothing ever arrives at; the wait gives up after limit_ns and the
+// kernel records kErrWaitTimeout and returns, leaving the context usable.
+// ========================================================================
+__global__ void wait_selftest_kernel(uint64_t limit_ns, int *status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0, limit_ns)) atomicOr(status, kErrWaitTimeout);
+}
+
+cudaError_t launch_wait_selftest(uint64_t limit_ns, int *status, cudaStream_t st) {
+  wait_selftest_kernel<<<1, 32, 0, st>>>(limit_ns, status);
+  return cudaGetLastError();
+}
+
+// ========================================================================
 // Cross-slice reduction: fixed slice order, so results are bit-stable.
 // ========================================================================
 __global__ void __launch_bounds__(256) reduce_kernel(ReduceArgs R) {

@@ -69,18 +69,22 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Waits for phase `parity` of `bar`, giving up after ~2 s of wall time.
+// Waits for phase `parity` of `bar`, giving up after `limit_ns` of wall
+// time (~2 s by default) or 2^22 rounds of 64 polls, whichever comes first.
 // Returns false on timeout; the caller records the error and carries on
 // without waiting again, so no thread can hang.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint64_t limit_ns = 2000000000ull) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
-  for (;;) {
+#pragma unroll 1
+  for (uint32_t round = 0; round < (1u << 22); round++) {
 #pragma unroll 1
     for (int k = 0; k < 64; k++)
       if (mbar_try(bar, parity)) return true;
-    if (global_timer_ns() - t0 > 2000000000ull) return false;
+    if (global_timer_ns() - t0 > limit_ns) return false;
   }
+  return false;
 }
 // Barrier among the `nthreads` consumer threads only (id 1; id 0 is
 // __syncthreads).

@@ -11,6 +11,7 @@ cudaError_t launch_predict(int order, int prec, int nj, double ti, const JState 
 cudaError_t launch_force(int order, int prec, const ForceArgs &A, int tpi, int ip,
                          cudaStream_t st);
 cudaError_t launch_reduce(const ReduceArgs &R, cudaStream_t st);
+cudaError_t launch_wait_selftest(uint64_t limit_ns, int *status, cudaStream_t st);
 cudaError_t launch_readj(int order, int first, int n, double ti, int predict, const JState &js,
                          double *out, cudaStream_t st);
 
