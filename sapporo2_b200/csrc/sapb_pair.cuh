@@ -188,11 +188,10 @@ struct Pre2 {
   float2 dx, dy, dz, inv;
 };
 
-// MASK = false drops the self-pair compare and select, for callers that
-// know no j has the id of either i.  (Choosing it per tile from the tiles'
-// id ranges measured 2 % slower on B200 than always masking: the two loop
-// copies cost more than the four ALU instructions they save.)
-template <bool MASK = true>
+// The self pair is masked on every pair (two compares and selects on the
+// ALU pipe): choosing an unmasked loop per tile from the tiles' id ranges
+// measured 2 % slower on B200, the two loop copies costing more than the
+// four ALU instructions they save.
 __device__ __forceinline__ Pre2 pair_mix2_pre(const IMix2 &I, const float4 &r0, const float4 &r1,
                                               float2 eps2, float2 &tmin) {
   Pre2 P;
@@ -200,11 +199,9 @@ __device__ __forceinline__ Pre2 pair_mix2_pre(const IMix2 &I, const float4 &r0, 
   P.dx = __fadd2_rn(__fadd2_rn(bc2(r0.x), I.nxh), __fadd2_rn(bc2(r1.x), I.nxl));
   P.dy = __fadd2_rn(__fadd2_rn(bc2(r0.y), I.nyh), __fadd2_rn(bc2(r1.y), I.nyl));
   P.dz = __fadd2_rn(__fadd2_rn(bc2(r0.z), I.nzh), __fadd2_rn(bc2(r1.z), I.nzl));
-  if (MASK) {
-    const int idj = __float_as_int(r1.w);
-    P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
-    P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
-  }
+  const int idj = __float_as_int(r1.w);
+  P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
+  P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
   const float2 ds2 = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dx, P.dx)));
   tmin.x = fminf(tmin.x, ds2.x);
   tmin.y = fminf(tmin.y, ds2.y);
@@ -255,11 +252,11 @@ __device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, fl
   }
 }
 
-template <int ORDER, bool MASK = true>
+template <int ORDER>
 __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, const float4 &r1,
                                           const float4 &r2, const float4 &r3, float2 eps2,
                                           AccMix2 &A, float2 &tmin) {
-  const Pre2 P = pair_mix2_pre<MASK>(I, r0, r1, eps2, tmin);
+  const Pre2 P = pair_mix2_pre(I, r0, r1, eps2, tmin);
   pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
 
