@@ -2,6 +2,7 @@
 into oracle/_ref, launched with the reference geometry) against this
 library's kernels on the same inputs and the same GPU: every (order,
 precision) pair must be faster here.  Times are printed (run with -s)."""
+import os
 import time
 
 import numpy as np
@@ -13,7 +14,8 @@ from tests import cases as T
 
 pytestmark = pytest.mark.gpu
 
-N = 32768  # all-i sweep: N^2 = 1.07e9 interactions per launch set
+# all-i sweep: N^2 interactions per launch (32768: 1.07e9); SAPB_REF_SPEED_N overrides
+N = int(os.environ.get("SAPB_REF_SPEED_N", "32768"))
 
 
 @pytest.mark.parametrize("order,precision", [(1, sp.DOUBLESINGLE), (1, sp.DOUBLE),
