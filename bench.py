@@ -470,8 +470,8 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=200)
     ap.add_argument("--launch", default=None,
                     help="force-kernel shape override tpi,ip,slices (default: planner)")
-    ap.add_argument("--only", choices=["all", "mixed"], default="all",
-                    help="mixed: time only the mixed-precision device arm (profiling runs)")
+    ap.add_argument("--only", choices=["all", "mixed", "fp64"], default="all",
+                    help="mixed / fp64: time only that device arm (profiling runs)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -519,6 +519,12 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.only == "fp64":  # profiling runs of the all-FP64 kernels
+        f = device_arm(cfg, sp.DOUBLE, args.steps, args.warmup, torch, flush, shard=shard)
+        print(json.dumps({"metric": "interactions/s, all-FP64 kernels", "unit": "interactions/s",
+                          "value": float(n) * n / (np.mean(f["force_ms"]) * 1e-3),
+                          "force_ms": float(np.mean(f["force_ms"])), "plan": f["plan"]}))
+        return
     clocks = ClockSampler(local)
     clocks.start()
     mix = device_arm(cfg, sp.DOUBLESINGLE, args.steps, args.warmup, torch, flush, shard=shard)

@@ -278,45 +278,55 @@ __device__ __forceinline__ double pair_dr_dp(const IDp &I, const double4 &r0, co
   return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
 }
 
+// rsqrt in FP64 for x in [FLT_MIN, FLT_MAX]: a 23-bit seed from the MUFU
+// (rsqrt.approx.ftz.f32 of x rounded to float) and two Newton-Raphson steps
+// y <- y (3/2 - x/2 y^2) in FP64 (quadratic convergence: 2^-22 -> 2^-44 ->
+// below 1 ulp before rounding).  x = +inf (the masked self pair) gives 0.
+__device__ __forceinline__ double rsqrt_nr64(double x) {
+  double y = (double)rsqrt_mufu(__double2float_rn(x));
+  const double hx = 0.5 * x;
+  y = y * fma(-hx, y * y, 1.5);
+  y = y * fma(-hx, y * y, 1.5);
+  return y;
+}
+
+// Same algebra as pair_mix: a3 = -3 alpha, b3 = -3 beta,
+//   jerk_ij = minv3 t,  t = dv + a3 dr
+//   snap_ij = minv3 (da + b3 dr + 2 a3 t)      (kernels.cu:642-667)
 template <int ORDER>
 __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const double4 &r1,
                                         const double4 &r2, double eps2, AccDp &A, double &tmin) {
   double dx, dy, dz;
   const double ds2 = pair_dr_dp(I, r0, r1, dx, dy, dz);
   tmin = fmin(tmin, ds2);
-  const double inv = rsqrt(ds2 + eps2);
-  const double minvr1 = r0.w * inv;
-  const double invr2 = inv * inv;
-  const double minvr3 = minvr1 * invr2;
-  A.ax += minvr3 * dx;
-  A.ay += minvr3 * dy;
-  A.az += minvr3 * dz;
-  A.pot += -minvr1;
+  const double inv = rsqrt_nr64(ds2 + eps2);
+  const double inv2 = inv * inv;
+  const double minv = r0.w * inv;
+  const double minv3 = minv * inv2;
+  A.ax = fma(minv3, dx, A.ax);
+  A.ay = fma(minv3, dy, A.ay);
+  A.az = fma(minv3, dz, A.az);
+  A.pot -= minv;
   const double dvx = r1.x - I.vx, dvy = r1.y - I.vy, dvz = r1.z - I.vz;
-  const double rv = dx * dvx + dy * dvy + dz * dvz;
+  const double rv = fma(dz, dvz, fma(dy, dvy, dx * dvx));
+  const double m3i2 = -3.0 * inv2;
+  const double a3 = m3i2 * rv;
   if (ORDER == FOURTH) {
-    const double drdv = (-3.0) * (minvr3 * invr2) * rv;
-    A.jx += minvr3 * dvx + drdv * dx;
-    A.jy += minvr3 * dvy + drdv * dy;
-    A.jz += minvr3 * dvz + drdv * dz;
+    A.jx = fma(minv3, fma(a3, dx, dvx), A.jx);
+    A.jy = fma(minv3, fma(a3, dy, dvy), A.jy);
+    A.jz = fma(minv3, fma(a3, dz, dvz), A.jz);
   } else {
     const double dax = r2.x - I.ax, day = r2.y - I.ay, daz = r2.z - I.az;
-    const double v2 = dvx * dvx + dvy * dvy + dvz * dvz;
-    const double ra = dx * dax + dy * day + dz * daz;
-    double alpha = rv * invr2;
-    double beta = (v2 + ra) * invr2 + alpha * alpha;
-    alpha *= -3.0;
-    const double ex = minvr3 * dvx + alpha * (minvr3 * dx);
-    const double ey = minvr3 * dvy + alpha * (minvr3 * dy);
-    const double ez = minvr3 * dvz + alpha * (minvr3 * dz);
-    alpha *= 2.0;
-    beta *= -3.0;
-    A.sx += minvr3 * dax + alpha * ex + beta * (minvr3 * dx);
-    A.sy += minvr3 * day + alpha * ey + beta * (minvr3 * dy);
-    A.sz += minvr3 * daz + alpha * ez + beta * (minvr3 * dz);
-    A.jx += ex;
-    A.jy += ey;
-    A.jz += ez;
+    const double s = fma(dz, daz, fma(dy, day, fma(dx, dax, fma(dvz, dvz, fma(dvy, dvy, dvx * dvx)))));
+    const double b3 = fma(a3, a3 * (-1.0 / 3.0), s * m3i2);
+    const double a6 = a3 + a3;
+    const double tx = fma(a3, dx, dvx), ty = fma(a3, dy, dvy), tz = fma(a3, dz, dvz);
+    A.jx = fma(minv3, tx, A.jx);
+    A.jy = fma(minv3, ty, A.jy);
+    A.jz = fma(minv3, tz, A.jz);
+    A.sx = fma(minv3, fma(a6, tx, fma(b3, dx, dax)), A.sx);
+    A.sy = fma(minv3, fma(a6, ty, fma(b3, dy, day)), A.sy);
+    A.sz = fma(minv3, fma(a6, tz, fma(b3, dz, daz)), A.sz);
   }
 }
 

@@ -75,3 +75,28 @@ def test_small_active_sets(gpu, ni):
     T.check_forces(got, want, 2)
     T.check_nn(case, got["nnb"], want, sel=sel)
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want, sel=sel)
+
+
+@pytest.mark.parametrize("eps2", [0.0, 1e-6])
+def test_fp64_kernel_rsqrt_over_scales(gpu, eps2):
+    """The FP64 kernels take 1/sqrt by Newton-Raphson from a MUFU seed: one j
+    at the origin, i at distances 1e-6 .. 1e2, against long-double sums."""
+    rng = np.random.default_rng(17)
+    n_i = 2000
+    d = 10.0 ** rng.uniform(-6, 2, n_i)
+    u = rng.normal(size=(n_i, 3))
+    xi = d[:, None] * u / np.linalg.norm(u, axis=1)[:, None]
+    with sp.Sapporo(order=sp.FOURTH, precision=sp.DOUBLE) as s:
+        z = np.zeros((1, 3))
+        s.set_j_particles([0], [0], [0.0], [1.0], z, z, z, z)
+        s.set_time(0.0)
+        s.start(1, np.arange(1, n_i + 1), xi, np.zeros((n_i, 3)), None, eps2, np.zeros(n_i))
+        got = s.results(1)
+    xl = xi.astype(np.longdouble)
+    r2 = (xl * xl).sum(1) + np.longdouble(eps2)
+    inv = 1 / np.sqrt(r2)
+    acc = (-xl * (inv ** 3)[:, None]).astype(np.float64)
+    pot = (-inv).astype(np.float64)
+    ea = np.linalg.norm(got["acc"] - acc, axis=1) / np.linalg.norm(acc, axis=1)
+    ep = np.abs(got["pot"] - pot) / np.abs(pot)
+    assert ea.max() < 2e-15 and ep.max() < 1e-15, (ea.max(), ep.max())
