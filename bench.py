@@ -130,6 +130,7 @@ def measured_peaks() -> dict:
 
 # ---------------------------------------------------------------------------
 LAUNCH = None  # (tpi, ip, slices) override for the force kernel, from --launch
+LAUNCH_PREC = None  # the precision the override applies to (mixed unless --only fp64)
 
 
 def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists=False,
@@ -152,7 +153,7 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
     # a dedicated stream: the library and the timing events must share it
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
-    if LAUNCH and precision == sp.DOUBLESINGLE:
+    if LAUNCH and precision == (LAUNCH_PREC if LAUNCH_PREC is not None else sp.DOUBLESINGLE):
         s.set_launch(*LAUNCH)
     s.set_j_particles(np.arange(nj), cfg["id"][jsel], cfg["t0"][jsel], cfg["m"][jsel],
                       cfg["x"][jsel], cfg["v"][jsel], cfg["a"][jsel], cfg["j"][jsel],
@@ -482,8 +483,9 @@ def main():
         run_reference(args, rank, world)
         return
     if args.launch:
-        global LAUNCH
+        global LAUNCH, LAUNCH_PREC
         LAUNCH = tuple(int(v) for v in args.launch.split(","))
+        LAUNCH_PREC = 2 if args.only == "fp64" else None  # 2 = DOUBLE
 
     import torch
     torch.cuda.set_device(local)

@@ -189,10 +189,9 @@ struct Plan {
   int tpi, ip, ns, i_tiles, slice_tiles;
 };
 
-static int blocks_per_sm(int order, int prec, int ip) {
-  if (prec == DOUBLE) return ip == 2 ? 3 : 4;
-  (void)order;
-  return ip >= 4 ? 2 : 4;  // mixed: <= 128 registers (ip 1, 2), <= 255 (ip 4)
+// resident blocks per SM of a force-kernel shape (occupancy API)
+static int blocks_per_sm(int order, int prec, int tpi, int ip) {
+  return std::max(1, force_blocks_per_sm(order, prec, tpi, ip));
 }
 
 // Launch shape for ni i-particles and nj j: threads-per-i, i per thread and
@@ -206,9 +205,16 @@ static int blocks_per_sm(int order, int prec, int ip) {
 static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   const int tj = force_tile_j();
   const int ntiles = std::max(1, (nj + tj - 1) / tj);
-  // mixed precision prefers 4 i per thread (two packed FP32x2 chains per j)
+  // (threads per i, i per thread) and the shape's throughput relative to the
+  // best one, measured on B200 at N = 2^20 (6th order, all i, where waves
+  // cost nothing): mixed (1,4) 537.8, (2,4) 534.6, (1,2) 521.8, (2,2) 516.1,
+  // (4,2) 510.4, (8,2) 491.2 G interactions/s; FP64 (2,2) 249.6, (4,2) 247.4,
+  // (8,2) 244.8, (1,2) 243.9.  The one-i-per-thread shapes (only chosen for
+  // very small ni) are estimates.
   static const int shapes_mix[][2] = {{1, 4}, {2, 4}, {1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
-  static const int shapes_dp[][2] = {{1, 2}, {2, 2}, {4, 2}, {8, 2}, {16, 1}, {32, 1}};
+  static const double eff_mix[] = {1.0, 0.994, 0.970, 0.960, 0.949, 0.913, 0.85, 0.85};
+  static const int shapes_dp[][2] = {{2, 2}, {4, 2}, {8, 2}, {1, 2}, {16, 1}, {32, 1}};
+  static const double eff_dp[] = {1.0, 0.991, 0.981, 0.977, 0.9, 0.9};
   const int nshape = d->prec == DOUBLE ? 6 : 8;
   // pair-times per SM and second (B200, measured order of magnitude): only
   // the balance between force and reduction depends on them
@@ -223,9 +229,9 @@ static Plan make_plan(const sapb_dev *d, int ni, int nj) {
     const int ip = d->ip ? d->ip : sh[1];
     const int ti = force_tile_i(tpi, ip);
     const int i_tiles = (ni + ti - 1) / ti;
-    const int bps = blocks_per_sm(d->order, d->prec, ip);
+    const int bps = blocks_per_sm(d->order, d->prec, tpi, ip);
     const long R = (long)d->num_sms * bps;
-    const double speed = ip >= 4 ? 1.0 : (ip == 2 ? 0.97 : 0.8);
+    const double speed = d->tpi ? 1.0 : (d->prec == DOUBLE ? eff_dp[q] : eff_mix[q]);
     const double tile_time = 128.0 * ti * bps / (speed * sm_rate);
     auto consider = [&](int ns) {
       ns = std::max(1, std::min(ns, max_ns));

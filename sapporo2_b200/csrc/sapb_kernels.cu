@@ -532,48 +532,80 @@ cudaError_t launch_predict(int order, int prec, int nj, double ti, const JState 
 }
 
 template <int ORDER, int PREC, int TPI, int IP>
-static cudaError_t launch_force_t(const ForceArgs &A, cudaStream_t st) {
+static cudaError_t launch_force_t(const ForceArgs *A, cudaStream_t st, int *occ) {
   using C = FCfg<ORDER, PREC, TPI, IP>;
   static bool attr_done = false;  // one-time attribute per instantiation
+  static int blocks_per_sm = 0;   // resident blocks per SM, from the occupancy API
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(force_kernel<ORDER, PREC, TPI, IP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  dim3 grid(A.i_tiles, A.nslices);
-  force_kernel<ORDER, PREC, TPI, IP><<<grid, kBT, C::SMEM, st>>>(A);
+  if (occ) {  // query only
+    if (!blocks_per_sm) {
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &blocks_per_sm, force_kernel<ORDER, PREC, TPI, IP>, kBT, C::SMEM);
+      if (e != cudaSuccess) return e;
+    }
+    *occ = blocks_per_sm;
+    return cudaSuccess;
+  }
+  dim3 grid(A->i_tiles, A->nslices);
+  force_kernel<ORDER, PREC, TPI, IP><<<grid, kBT, C::SMEM, st>>>(*A);
   return cudaGetLastError();
 }
 
+// Launches (occ == nullptr) or reports the resident blocks per SM (occ) of
+// one instantiation.
 template <int ORDER, int PREC>
-static cudaError_t launch_force_o(const ForceArgs &A, int tpi, int ip, cudaStream_t st) {
+static cudaError_t launch_force_o(const ForceArgs *A, int tpi, int ip, cudaStream_t st, int *occ) {
   if (ip == 4 && PREC != DOUBLE) {
     switch (tpi) {
-      case 1: return launch_force_t<ORDER, PREC, 1, 4>(A, st);
-      case 2: return launch_force_t<ORDER, PREC, 2, 4>(A, st);
+      case 1: return launch_force_t<ORDER, PREC, 1, 4>(A, st, occ);
+      case 2: return launch_force_t<ORDER, PREC, 2, 4>(A, st, occ);
       default: break;
     }
   } else if (ip == 2) {
     switch (tpi) {
-      case 1: return launch_force_t<ORDER, PREC, 1, 2>(A, st);
-      case 2: return launch_force_t<ORDER, PREC, 2, 2>(A, st);
-      case 4: return launch_force_t<ORDER, PREC, 4, 2>(A, st);
-      case 8: return launch_force_t<ORDER, PREC, 8, 2>(A, st);
+      case 1: return launch_force_t<ORDER, PREC, 1, 2>(A, st, occ);
+      case 2: return launch_force_t<ORDER, PREC, 2, 2>(A, st, occ);
+      case 4: return launch_force_t<ORDER, PREC, 4, 2>(A, st, occ);
+      case 8: return launch_force_t<ORDER, PREC, 8, 2>(A, st, occ);
       default: break;
     }
   } else if (ip == 1) {
     switch (tpi) {
-      case 1: return launch_force_t<ORDER, PREC, 1, 1>(A, st);
-      case 2: return launch_force_t<ORDER, PREC, 2, 1>(A, st);
-      case 4: return launch_force_t<ORDER, PREC, 4, 1>(A, st);
-      case 8: return launch_force_t<ORDER, PREC, 8, 1>(A, st);
-      case 16: return launch_force_t<ORDER, PREC, 16, 1>(A, st);
-      case 32: return launch_force_t<ORDER, PREC, 32, 1>(A, st);
+      case 1: return launch_force_t<ORDER, PREC, 1, 1>(A, st, occ);
+      case 2: return launch_force_t<ORDER, PREC, 2, 1>(A, st, occ);
+      case 4: return launch_force_t<ORDER, PREC, 4, 1>(A, st, occ);
+      case 8: return launch_force_t<ORDER, PREC, 8, 1>(A, st, occ);
+      case 16: return launch_force_t<ORDER, PREC, 16, 1>(A, st, occ);
+      case 32: return launch_force_t<ORDER, PREC, 32, 1>(A, st, occ);
       default: break;
     }
   }
   return cudaErrorInvalidConfiguration;
+}
+
+static cudaError_t force_dispatch(int order, int prec, const ForceArgs *A, int tpi, int ip,
+                                  cudaStream_t st, int *occ) {
+  if (order == FOURTH && prec == DOUBLESINGLE)
+    return launch_force_o<FOURTH, DOUBLESINGLE>(A, tpi, ip, st, occ);
+  if (order == FOURTH && prec == DOUBLE) return launch_force_o<FOURTH, DOUBLE>(A, tpi, ip, st, occ);
+  if (order == SIXTH && prec == DOUBLESINGLE)
+    return launch_force_o<SIXTH, DOUBLESINGLE>(A, tpi, ip, st, occ);
+  if (order == SIXTH && prec == DOUBLE) return launch_force_o<SIXTH, DOUBLE>(A, tpi, ip, st, occ);
+  return cudaErrorInvalidValue;
+}
+
+int force_blocks_per_sm(int order, int prec, int tpi, int ip) {
+  int n = 0;
+  if (force_dispatch(order, prec, nullptr, tpi, ip, 0, &n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
 }
 
 int force_tile_i(int tpi, int ip) { return (kBT / tpi) * ip; }
@@ -581,13 +613,7 @@ int force_tile_j() { return kTJ; }
 
 cudaError_t launch_force(int order, int prec, const ForceArgs &A, int tpi, int ip,
                          cudaStream_t st) {
-  if (order == FOURTH && prec == DOUBLESINGLE)
-    return launch_force_o<FOURTH, DOUBLESINGLE>(A, tpi, ip, st);
-  if (order == FOURTH && prec == DOUBLE) return launch_force_o<FOURTH, DOUBLE>(A, tpi, ip, st);
-  if (order == SIXTH && prec == DOUBLESINGLE)
-    return launch_force_o<SIXTH, DOUBLESINGLE>(A, tpi, ip, st);
-  if (order == SIXTH && prec == DOUBLE) return launch_force_o<SIXTH, DOUBLE>(A, tpi, ip, st);
-  return cudaErrorInvalidValue;
+  return force_dispatch(order, prec, &A, tpi, ip, st, nullptr);
 }
 
 cudaError_t launch_readj(int order, int first, int n, double ti, int predict, const JState &js,

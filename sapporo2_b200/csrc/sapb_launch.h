@@ -24,6 +24,9 @@ cudaError_t launch_batch(int order, int prec, const BatchArgs &B, int j_grid, in
 int batch_blocks_per_sm(int order, int prec);  // resident persistent blocks per SM
 
 int force_tile_i(int tpi, int ip);  // i-particles per block
+// resident blocks per SM of one force-kernel instantiation (occupancy API,
+// cached; 0 if the shape does not exist)
+int force_blocks_per_sm(int order, int prec, int tpi, int ip);
 int force_tile_j();                  // j records per tile
 
 }  // namespace sapb
