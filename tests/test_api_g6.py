@@ -1,0 +1,46 @@
+"""GPU: the GRAPE-6 interface (g6_*, lib/interfaces/sapporoG6lib.cpp) against
+the FP64 oracle: a2/j6 scaling of the stored j, forces, the nearest
+neighbour of g6calc_lasthalf2_, and the neighbour-list readout."""
+import numpy as np
+import pytest
+
+import sapporo2_b200 as sp
+from tests import cases as T
+
+pytestmark = pytest.mark.gpu
+
+
+def test_g6_forces_nn_and_lists(gpu):
+    case = T.build_case(1, 2000, seed=101, binaries=0.1)
+    n = case["n"]
+    g6 = sp.G6()
+    assert g6.open_special((0,)) == 0
+    try:
+        assert g6.npipes() >= n
+        z3 = np.zeros(3)
+        for k in range(n):
+            # GRAPE-6 stores a2 = a/2 and j6 = jerk/6 (sapporoG6lib.cpp:102-104)
+            g6.set_j_particle(k, int(case["id"][k]), float(case["t0"][k]), 0.0,
+                              float(case["m"][k]), z3, case["j"][k] / 6.0, case["a"][k] / 2.0,
+                              case["v"][k], case["x"][k])
+        g6.set_ti(case["ti"])
+        ids = case["id"]
+        zi = np.zeros((n, 3))
+        g6.calc_firsthalf(n, ids, case["px"], case["pv"], zi, zi, np.zeros(n), case["eps2"],
+                          case["h2"])
+        rc, acc, jrk, pot, inn = g6.calc_lasthalf2(n, ids, case["px"], case["pv"],
+                                                   case["eps2"], case["h2"])
+        assert rc == 0
+        ovf = g6.read_neighbour_list()
+        lists = [g6.get_neighbour_list(i, sp.NGB_PB) for i in range(n)]
+    finally:
+        g6.close()
+    want = T.oracle_force(case)
+    T.check_forces({"acc": acc, "jrk": jrk, "pot": pot}, want, 1)
+    T.check_nn(case, inn, want)
+    assert ovf == int(np.any(want["ngb_count"] >= sp.NGB_PB))
+    counts = np.array([q[1] for q in lists])
+    np.testing.assert_array_equal(counts, want["ngb_count"])
+    for q in lists:
+        assert np.all(np.diff(q[2]) > 0)  # sorted, as get_ngb_list returns them
+    T.check_neighbours(case, [q[2] for q in lists], counts, want)
