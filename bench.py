@@ -377,6 +377,7 @@ def run_learned_h2_bench(args):
             "ms_per_step": 1e3 * st["step_s"] / max(st["steps"], 1),
             "force_ms_per_step": 1e3 * st["force_s"] / max(st["steps"], 1),
             "train_ms_per_step": 1e3 * getattr(sim.policy, "train_s", 0.0) / max(st["steps"], 1),
+            "propose_ms_per_step": 1e3 * getattr(sim.policy, "propose_s", 0.0) / max(st["steps"], 1),
             "pretrain_s": getattr(sim.policy, "pretrain_s", 0.0),
             "init_s": t_init, "t_end": float(sim.t.max()), "rel_energy_error": de,
             "mean_active": float(np.mean(active)),

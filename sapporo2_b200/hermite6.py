@@ -63,19 +63,21 @@ class LearnedH2:
     """The GPU-trained network proposes h2 from the particle's previous
     evaluation (as a correction to the count-scaled radius).  It is
     pretrained on the counts of the two start-up force passes (two radii)
-    and then learns from every first-attempt count."""
+    and then learns online from first-attempt counts."""
 
     name = "learned"
 
     def __init__(self, sap, seed=5, epochs=4, lr=1e-3, pre_epochs=300, max_batch=8192,
-                 max_pre=65536):
+                 max_pre=65536, train_every=4):
         self.net = H2Net(sap, seed=seed)
         self.epochs, self.lr, self.pre_epochs = epochs, lr, pre_epochs
-        self.max_batch, self.max_pre = max_batch, max_pre
+        self.max_batch, self.max_pre, self.train_every = max_batch, max_pre, train_every
         self.rng = np.random.default_rng(seed)
         self.losses = []
         self.train_s = 0.0
         self.pretrain_s = 0.0
+        self.propose_s = 0.0
+        self.n_obs = 0
 
     def start(self, sim, samples):
         t0 = time.perf_counter()
@@ -90,11 +92,17 @@ class LearnedH2:
         self.pretrain_s += time.perf_counter() - t0
 
     def propose(self, sim, idx):
-        return self.net.propose(sim.n_prev[idx], sim.h2_prev[idx], sim.a[idx], sim.j[idx])
+        t0 = time.perf_counter()
+        h2 = self.net.propose(sim.n_prev[idx], sim.h2_prev[idx], sim.a[idx], sim.j[idx])
+        self.propose_s += time.perf_counter() - t0
+        return h2
 
     def observe(self, sim, idx, h2_used, counts):
         """One online update on (at most max_batch of) this step's first
-        attempts."""
+        attempts, every train_every-th block step."""
+        self.n_obs += 1
+        if (self.n_obs - 1) % self.train_every:
+            return
         t0 = time.perf_counter()
         take = np.arange(len(idx))
         if len(take) > self.max_batch:
