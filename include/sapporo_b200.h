@@ -55,7 +55,11 @@ int sapb_device_count(int *count);
  * sapporo::open (lib/src/sapporohostclass.cpp:90-372) together with
  * device::assignDevice / allocateMemory (lib/include/sapdevclass.h:122-273).
  * n_pipes: maximum i per force call (<= 0: SAPB_NPIPES);
- * nj_reserve: initial j capacity (<= 0: 16384, as the reference). */
+ * nj_reserve: initial j capacity (<= 0: 16384, as the reference).
+ * order SAPB_GRAPE5 (mixed precision): acceleration and potential only, every
+ * pair including the self pair, no nearest neighbour or lists (the
+ * reference's GRAPE5 kernels, kernels.cu:565, :1096-1098); with DOUBLE it
+ * runs the 4th-order FP64 kernels.  Storage is the 4th-order layout. */
 int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
               int nj_reserve);
 int sapb_close(sapb_dev *d);

@@ -4,9 +4,10 @@
  * positions and masses only, acceleration and potential out, no ids.  As on
  * GRAPE-5 the self pair is not skipped: it adds -m_i/eps to the potential of
  * an i that coincides with a j (and nothing to the acceleration).  Computed
- * by the 4th-order mixed-precision kernels with zero velocities (the jerk is
- * dropped).  Void calls that the reference ends with exit() (softening or nj
- * not set) report on stderr and return without computing.
+ * by the GRAPE-5 mixed-precision kernels (double-single position
+ * difference, no jerk, no neighbour search).  Void calls that the reference
+ * ends with exit() (softening or nj not set) report on stderr and return
+ * without computing.
  */
 #ifndef SAPPORO_G5_H
 #define SAPPORO_G5_H

@@ -363,6 +363,7 @@ static cudaError_t launch_batch_t(const BatchArgs &B, int j_grid, int force_bloc
 
 cudaError_t launch_batch(int order, int prec, const BatchArgs &B, int j_grid, int force_blocks,
                          int i_grid, cudaStream_t st) {
+  if (order == GRAPE5) order = FOURTH;  // GRAPE-5 batches run the 4th-order kernels
   if (order == FOURTH && prec == DOUBLESINGLE)
     return launch_batch_t<FOURTH, DOUBLESINGLE>(B, j_grid, force_blocks, i_grid, st);
   if (order == FOURTH && prec == DOUBLE)
@@ -388,6 +389,7 @@ static int batch_occ_t() {
 }
 
 int batch_blocks_per_sm(int order, int prec) {
+  if (order == GRAPE5) order = FOURTH;
   if (order == FOURTH && prec == DOUBLESINGLE) return batch_occ_t<FOURTH, DOUBLESINGLE>();
   if (order == FOURTH && prec == DOUBLE) return batch_occ_t<FOURTH, DOUBLE>();
   if (order == SIXTH && prec == DOUBLESINGLE) return batch_occ_t<SIXTH, DOUBLESINGLE>();

@@ -325,8 +325,9 @@ int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
               int nj_reserve) {
   if (!out) return fail(nullptr, SAPB_EINVAL, "null handle pointer");
   *out = nullptr;
-  if (order != FOURTH && order != SIXTH)
-    return fail(nullptr, SAPB_EINVAL, "order %d not supported (4th=1, 6th=2)", order);
+  if (order != GRAPE5 && order != FOURTH && order != SIXTH)
+    return fail(nullptr, SAPB_EINVAL, "order %d not supported (GRAPE-5=0, 4th=1, 6th=2)",
+                order);
   if (precision != DOUBLESINGLE && precision != DOUBLE)
     return fail(nullptr, SAPB_EINVAL, "precision %d not supported (DS=1, DOUBLE=2)", precision);
   int ndev = 0;

@@ -333,13 +333,15 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           t[8 * kBT] += (double)P[p].sy;
           t[9 * kBT] += (double)P[p].sz;
         }
-        if (tmin[p] < best[p]) {
-          best[p] = tmin[p];
-          best_tile[p] = it;
+        if (ORDER != GRAPE5) {  // GRAPE-5: no nearest neighbour, no lists
+          if (tmin[p] < best[p]) {
+            best[p] = tmin[p];
+            best_tile[p] = it;
+          }
+          if (A.do_list)
+            list_rescan_mix<C::RS>(Im[p], tmin[p] < Im[p].h2, gi[p], ty, TPI, rec, cnt, lane,
+                                   A.ngb_count, A.ngb_list);
         }
-        if (A.do_list)
-          list_rescan_mix<C::RS>(Im[p], tmin[p] < Im[p].h2, gi[p], ty, TPI, rec, cnt, lane,
-                                 A.ngb_count, A.ngb_list);
       }
     }
     __syncwarp();
@@ -500,6 +502,7 @@ static cudaError_t launch_scatter_t(const double *stage, int n, int cap, const J
 
 cudaError_t launch_scatter(int order, int prec, const double *stage, int n, int cap,
                            const JState &js, void *pred, int *status, cudaStream_t st) {
+  if (order == GRAPE5) order = FOURTH;  // GRAPE-5 keeps the 4th-order layout
   if (order == FOURTH && prec == DOUBLESINGLE)
     return launch_scatter_t<FOURTH, DOUBLESINGLE>(stage, n, cap, js, pred, status, st);
   if (order == FOURTH && prec == DOUBLE)
@@ -521,6 +524,7 @@ static cudaError_t launch_predict_t(int nj, double ti, const JState &js, void *p
 
 cudaError_t launch_predict(int order, int prec, int nj, double ti, const JState &js, void *pred,
                            cudaStream_t st) {
+  if (order == GRAPE5) order = FOURTH;  // GRAPE-5 keeps the 4th-order layout
   if (order == FOURTH && prec == DOUBLESINGLE)
     return launch_predict_t<FOURTH, DOUBLESINGLE>(nj, ti, js, pred, st);
   if (order == FOURTH && prec == DOUBLE)
@@ -591,6 +595,9 @@ static cudaError_t launch_force_o(const ForceArgs *A, int tpi, int ip, cudaStrea
 
 static cudaError_t force_dispatch(int order, int prec, const ForceArgs *A, int tpi, int ip,
                                   cudaStream_t st, int *occ) {
+  if (order == GRAPE5 && prec == DOUBLESINGLE)
+    return launch_force_o<GRAPE5, DOUBLESINGLE>(A, tpi, ip, st, occ);
+  if (order == GRAPE5) order = FOURTH;  // FP64 GRAPE-5 calls run the 4th-order kernels
   if (order == FOURTH && prec == DOUBLESINGLE)
     return launch_force_o<FOURTH, DOUBLESINGLE>(A, tpi, ip, st, occ);
   if (order == FOURTH && prec == DOUBLE) return launch_force_o<FOURTH, DOUBLE>(A, tpi, ip, st, occ);

@@ -112,9 +112,16 @@ template <int ORDER>
 __device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const float4 &r1,
                                          const float4 &r2, const float4 &r3, float eps2,
                                          AccMix &A, float &tmin) {
-  float dx, dy, dz;
-  const float ds2 = pair_dr_mix(I, r0, r1, dx, dy, dz);
-  tmin = fminf(tmin, ds2);
+  float dx, dy, dz, ds2;
+  if (ORDER == GRAPE5) {  // every pair, the self pair included (kernels.cu:565)
+    dx = ds_sub(r0.x, r1.x, I.xh, I.xl);
+    dy = ds_sub(r0.y, r1.y, I.yh, I.yl);
+    dz = ds_sub(r0.z, r1.z, I.zh, I.zl);
+    ds2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+  } else {
+    ds2 = pair_dr_mix(I, r0, r1, dx, dy, dz);
+    tmin = fminf(tmin, ds2);
+  }
   const float inv = rsqrt_mufu(ds2 + eps2);
   const float inv2 = inv * inv;
   const float minv = r0.w * inv;
@@ -123,6 +130,7 @@ __device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const 
   A.ay = fmaf(minv3, dy, A.ay);
   A.az = fmaf(minv3, dz, A.az);
   A.pot -= minv;
+  if (ORDER == GRAPE5) return;  // acceleration and potential only
   const float dvx = r2.x - I.vx, dvy = r2.y - I.vy, dvz = r2.z - I.vz;
   const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
   const float m3i2 = -3.0f * inv2;
@@ -192,6 +200,7 @@ struct Pre2 {
 // ALU pipe): choosing an unmasked loop per tile from the tiles' id ranges
 // measured 2 % slower on B200, the two loop copies costing more than the
 // four ALU instructions they save.
+template <bool NGB = true>  // false (GRAPE-5): no self-pair mask, no nearest-neighbour minimum
 __device__ __forceinline__ Pre2 pair_mix2_pre(const IMix2 &I, const float4 &r0, const float4 &r1,
                                               float2 eps2, float2 &tmin) {
   Pre2 P;
@@ -199,12 +208,16 @@ __device__ __forceinline__ Pre2 pair_mix2_pre(const IMix2 &I, const float4 &r0, 
   P.dx = __fadd2_rn(__fadd2_rn(bc2(r0.x), I.nxh), __fadd2_rn(bc2(r1.x), I.nxl));
   P.dy = __fadd2_rn(__fadd2_rn(bc2(r0.y), I.nyh), __fadd2_rn(bc2(r1.y), I.nyl));
   P.dz = __fadd2_rn(__fadd2_rn(bc2(r0.z), I.nzh), __fadd2_rn(bc2(r1.z), I.nzl));
-  const int idj = __float_as_int(r1.w);
-  P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
-  P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
+  if (NGB) {
+    const int idj = __float_as_int(r1.w);
+    P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
+    P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
+  }
   const float2 ds2 = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dx, P.dx)));
-  tmin.x = fminf(tmin.x, ds2.x);
-  tmin.y = fminf(tmin.y, ds2.y);
+  if (NGB) {
+    tmin.x = fminf(tmin.x, ds2.x);
+    tmin.y = fminf(tmin.y, ds2.y);
+  }
   const float2 r2v = __fadd2_rn(ds2, eps2);
   P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
   return P;
@@ -222,6 +235,7 @@ __device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, fl
   A.ay = __ffma2_rn(minv3, dy, A.ay);
   A.az = __ffma2_rn(minv3, dz, A.az);
   A.pot = __fadd2_rn(A.pot, minv);
+  if (ORDER == GRAPE5) return;  // acceleration and potential only
   const float2 dvx = __fadd2_rn(bc2(r2.x), I.nvx);
   const float2 dvy = __fadd2_rn(bc2(r2.y), I.nvy);
   const float2 dvz = __fadd2_rn(bc2(r2.z), I.nvz);
@@ -256,7 +270,7 @@ template <int ORDER>
 __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, const float4 &r1,
                                           const float4 &r2, const float4 &r3, float2 eps2,
                                           AccMix2 &A, float2 &tmin) {
-  const Pre2 P = pair_mix2_pre(I, r0, r1, eps2, tmin);
+  const Pre2 P = pair_mix2_pre<ORDER != GRAPE5>(I, r0, r1, eps2, tmin);
   pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
 

@@ -1,9 +1,8 @@
 // GRAPE-5 C interface over one process-wide `sapporo` instance, as the
 // reference's lib/interfaces/sapporoG5lib.cpp (declared in
-// include/sapporo_g5.h).  GRAPE-5 has no ids and no velocities: the j get
-// their address as id and zero velocity, the i get an id no j carries, so
-// the self pair is computed as on GRAPE-5 (kernels.cu:565 does not skip it
-// for GRAPE5): zero force, -m/eps potential.
+// include/sapporo_g5.h).  Opened in GRAPE5 order: the kernels compute
+// acceleration and potential only, over every pair including the self pair
+// (kernels.cu:565 does not skip it for GRAPE5: zero force, -m/eps potential).
 #include <limits.h>
 #include <stdio.h>
 
@@ -15,16 +14,10 @@
 static sapporo grav5;
 static int nj_to_use = -1;       // :31
 static double eps_to_use = -1;   // :32
-static std::vector<int> no_id;   // i ids: never equal to a j address
-static std::vector<double> zeros3, zeros1, jerk_scratch;
+static std::vector<double> h2_zero;  // h2 = 0: no neighbour lists
 
 static void reserve_i(int ni) {
-  if ((int)no_id.size() < ni) {
-    no_id.assign((size_t)ni, INT_MIN);
-    zeros3.assign((size_t)ni * 3, 0.0);
-    zeros1.assign((size_t)ni, 0.0);
-    jerk_scratch.assign((size_t)ni * 3, 0.0);
-  }
+  if ((int)h2_zero.size() < ni) h2_zero.assign((size_t)ni, 0.0);
 }
 
 static bool ready(const char *what) {
@@ -44,7 +37,7 @@ extern "C" {
 int g5_open_special(int ndev, int *list) {
   nj_to_use = -1;
   eps_to_use = -1;
-  const int rc = grav5.open("linked-in kernels", list, ndev, FOURTH, DOUBLESINGLE);
+  const int rc = grav5.open("linked-in kernels", list, ndev, GRAPE5, DOUBLESINGLE);
   if (rc == 0) reserve_i(grav5.get_n_pipes());
   return rc;
 }
@@ -88,9 +81,8 @@ void g5_set_jp(int addr, int nj, double jmass[], double xj[][3]) {
 void g5_set_xi(int ni, double xi[][3]) {
   if (!ready("g5_set_xi") || ni <= 0) return;
   reserve_i(ni);
-  grav5.startGravCalc(nj_to_use, ni, no_id.data(), xi,
-                      reinterpret_cast<double(*)[3]>(zeros3.data()), nullptr, nullptr, nullptr,
-                      eps_to_use, zeros1.data(), nullptr);
+  grav5.startGravCalc(nj_to_use, ni, nullptr, xi, nullptr, nullptr, nullptr, nullptr,
+                      eps_to_use, h2_zero.data(), nullptr);
 }
 
 void g5_run(void) {}
@@ -98,9 +90,8 @@ void g5_run(void) {}
 void g5_get_force(int ni, double a[][3], double *phi) {
   if (!ready("g5_get_force") || ni <= 0) return;
   reserve_i(ni);
-  double(*jrk)[3] = reinterpret_cast<double(*)[3]>(jerk_scratch.data());  // dropped
-  grav5.getGravResults(nj_to_use, ni, nullptr, nullptr, nullptr, 0, nullptr, a, jrk, nullptr,
-                       nullptr, phi, nullptr, nullptr, false);
+  grav5.getGravResults(nj_to_use, ni, nullptr, nullptr, nullptr, 0, nullptr, a, nullptr,
+                       nullptr, nullptr, phi, nullptr, nullptr, false);
 }
 
 void g5_calculate_force_on_x(double xi[][3], double a[][3], double *phi, int ni) {

@@ -15,6 +15,7 @@
 // more than NGB_PB entries and flags overflow when the count reaches NGB_PB.
 #include "../../include/sapporohostclass.h"
 
+#include <climits>
 #include <cmath>
 #include <cstdint>
 
@@ -236,10 +237,11 @@ void sapporo::startGravCalc(int nj, int ni, int id[], double xi[][3], double vi[
     r[1] = xi[i][1];
     r[2] = xi[i][2];
     r[3] = h2 ? h2[i] : 0.0;
-    r[4] = vi[i][0];
-    r[5] = vi[i][1];
-    r[6] = vi[i][2];
-    put_int_pair(&r[7], id[i], 0);
+    // GRAPE-5 callers pass no velocities and no ids (sapporohostclass.cpp:617-633)
+    r[4] = vi ? vi[i][0] : 0.0;
+    r[5] = vi ? vi[i][1] : 0.0;
+    r[6] = vi ? vi[i][2] : 0.0;
+    put_int_pair(&r[7], id ? id[i] : INT_MIN, 0);
     if (integrationOrder > FOURTH) {
       r[8] = a[i][0];
       r[9] = a[i][1];
