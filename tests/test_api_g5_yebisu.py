@@ -95,3 +95,23 @@ def test_yebisu_api_forces_and_predictor(gpu):
     T.check_nn(case, f["nnb"], want)
     ok = want["nnb"] == f["nnb"]
     np.testing.assert_allclose(f["r2"][ok], want["ds2min"][ok].astype(np.float32), rtol=1e-6)
+
+
+@gpu
+def test_grape5_order_keeps_the_self_pair_whatever_the_ids(gpu):
+    """Order GRAPE5 through the class: ids are passed and equal the j ids,
+    yet, as on GRAPE-5, the self pair is not skipped and no neighbour is
+    searched."""
+    case = T.build_case(1, 1500, seed=93)
+    n, eps2 = case["n"], 1e-6
+    x, m = case["x"], case["m"]
+    z = np.zeros((n, 3))
+    with sp.Sapporo(order=sp.GRAPE5, precision=sp.DOUBLESINGLE) as s:
+        s.set_j_particles(np.arange(n), case["id"], np.zeros(n), m, x, z, z, z)
+        s.start(n, case["id"], x, z, None, eps2, np.full(n, 1.0))
+        got = s.results(n)
+        counts = s.neighbour_counts()
+    want = O.force(1, x, z, None, np.zeros(n), np.full(n, -7, dtype=np.int32), x, z, None, m,
+                   case["id"], eps2, lists=False)
+    T.check_forces({"acc": got["acc"], "pot": got["pot"]}, want, 1, fields=["acc", "pot"])
+    assert np.all(got["nnb"] == 0) and np.all(counts == 0)
