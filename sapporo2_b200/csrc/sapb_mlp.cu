@@ -11,6 +11,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <vector>
 
@@ -76,113 +77,226 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(const float *__restric
 }
 
 // Gradient of L = 1/(2n) sum (y - t)^2 over the n samples, accumulated into
-// G (zeroed by the caller), loss accumulated into *loss.  Block b handles
-// samples [128 b, 128 b + 128): activations and deltas are kept transposed
-// in shared memory ([unit][sample]) and each weight gradient is the block's
-// sum of outer products, added to G with one atomic per parameter.
-__global__ void __launch_bounds__(kMB) mlp_backward_kernel(const float *__restrict__ P, int n,
-                                                           const float *__restrict__ X,
-                                                           const float *__restrict__ T,
-                                                           float *__restrict__ G,
-                                                           float *__restrict__ loss) {
-  extern __shared__ float sm[];
-  float *sp = sm;                  // parameters  kNP
-  float *XS = sp + kNP;            // [5][128]
-  float *H1 = XS + kIn * kMB;      // [64][128]
-  float *H2 = H1 + kH * kMB;       // [64][128]
-  float *H3 = H2 + kH * kMB;       // [64][128]  (later: delta of layer 2)
-  float *D3 = H3 + kH * kMB;       // [64][128]  (later: delta of layer 1)
-  float *DY = D3 + kH * kMB;       // [128]
-  const int tid = threadIdx.x;
-  for (int k = tid; k < kNP; k += kMB) sp[k] = P[k];
-  const int i = blockIdx.x * kMB + tid;
-  const bool valid = i < n;
-  float x[kIn] = {0, 0, 0, 0, 0};
-  if (valid)
-    for (int k = 0; k < kIn; k++) x[k] = X[(size_t)i * kIn + k];
+// G (zeroed by the caller), loss accumulated into *loss.
+//
+// Persistent: each block loops over chunks of 128 samples (one per thread)
+// and keeps its share of the gradient in registers until the end, so G
+// receives one atomic per parameter per block (not per chunk).  Within a
+// chunk the activations and deltas sit in shared memory as [sample][unit]
+// rows padded to kS floats; every weight gradient is a sum over samples of
+// outer products, computed as register tiles (4 output units x 8 input units
+// per thread for the 64x64 layers: 3 vector shared loads per 32 FMA), and the
+// back-propagated deltas read the weight rows as float4 (one vector load per
+// 4 FMA, broadcast to the warp).
+constexpr int kS = 68;  // padded row: float4-aligned, conflict-free columns
+constexpr int kNPp = (kNP + 3) / 4 * 4;
+constexpr int kBwdFloats = kNPp + kMB * 8 + 4 * kMB * kS + kMB;
+
+__device__ __forceinline__ float4 ld4(const float *p) {
+  return *reinterpret_cast<const float4 *>(p);
+}
+
+__global__ void __launch_bounds__(kMB, 1) mlp_backward_kernel(const float *__restrict__ P, int n,
+                                                              const float *__restrict__ X,
+                                                              const float *__restrict__ T,
+                                                              float *__restrict__ G,
+                                                              float *__restrict__ loss) {
+  extern __shared__ __align__(16) float sm[];
+  float *sp = sm;                  // parameters (kNP, padded)
+  float *XS = sp + kNPp;           // [128][8]
+  float *A1 = XS + kMB * 8;        // [128][kS] post-ReLU layer 1
+  float *A2 = A1 + kMB * kS;       // [128][kS] post-ReLU layer 2
+  float *A3 = A2 + kMB * kS;       // [128][kS] post-ReLU layer 3, then delta 2
+  float *D3 = A3 + kMB * kS;       // [128][kS] delta 3, then delta 1
+  float *DY = D3 + kMB * kS;       // [128]
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  for (int k = t; k < kNP; k += kMB) sp[k] = P[k];
+
+  // register-tile owners: 4 output rows x 8 input columns of W2 and W3
+  const int o0 = (t >> 3) * 4, k0 = (t & 7) * 8;
+  float gW3[4][8], gW2[4][8];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 8; c++) gW3[r][c] = gW2[r][c] = 0.f;
+  float gW1[kIn] = {0, 0, 0, 0, 0};  // row t (t < 64)
+  float gB1 = 0.f, gB2 = 0.f, gB3 = 0.f, gW4 = 0.f, gB4 = 0.f;
+  float lsum = 0.f;
   __syncthreads();
-  float h1[kH], h2[kH], h3[kH];
-  const float y = mlp_eval(sp, x, h1, h2, h3);
-  const float dy = valid ? (y - T[i]) / (float)n : 0.f;
-  if (valid) atomicAdd(loss, 0.5f * (y - T[i]) * (y - T[i]) / (float)n);
-  for (int k = 0; k < kIn; k++) XS[k * kMB + tid] = valid ? x[k] : 0.f;
-  for (int k = 0; k < kH; k++) {
-    H1[k * kMB + tid] = valid ? h1[k] : 0.f;
-    H2[k * kMB + tid] = valid ? h2[k] : 0.f;
-    H3[k * kMB + tid] = valid ? h3[k] : 0.f;
-    // delta of layer 3 pre-activation: dy * W4 * relu'
-    D3[k * kMB + tid] = (valid && h3[k] > 0.f) ? dy * sp[oW4 + k] : 0.f;
+
+  const int nchunks = (n + kMB - 1) / kMB;
+  for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int i = chunk * kMB + t;
+    const bool valid = i < n;
+    // ---- forward for this thread's sample ----
+    float x[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; k++) x[k] = valid ? X[(size_t)i * kIn + k] : 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) XS[t * 8 + k] = k < kIn ? x[k] : 0.f;
+#pragma unroll 4
+    for (int o = 0; o < kH; o++) {
+      float s = sp[oB1 + o];
+#pragma unroll
+      for (int k = 0; k < kIn; k++) s = fmaf(sp[oW1 + o * kIn + k], x[k], s);
+      A1[t * kS + o] = fmaxf(s, 0.f);
+    }
+    // layers 2 and 3 read this thread's previous-layer row back as float4
+    // (activations stay out of the registers, which hold the gradient tiles)
+#pragma unroll 2
+    for (int o = 0; o < kH; o++) {
+      float s = sp[oB2 + o];
+#pragma unroll
+      for (int k = 0; k < kH; k += 4) {
+        const float4 w = ld4(sp + oW2 + o * kH + k);
+        const float4 h = ld4(A1 + t * kS + k);
+        s = fmaf(w.x, h.x, fmaf(w.y, h.y, fmaf(w.z, h.z, fmaf(w.w, h.w, s))));
+      }
+      A2[t * kS + o] = fmaxf(s, 0.f);
+    }
+    float y = sp[oB4];
+#pragma unroll 2
+    for (int o = 0; o < kH; o++) {
+      float s = sp[oB3 + o];
+#pragma unroll
+      for (int k = 0; k < kH; k += 4) {
+        const float4 w = ld4(sp + oW3 + o * kH + k);
+        const float4 h = ld4(A2 + t * kS + k);
+        s = fmaf(w.x, h.x, fmaf(w.y, h.y, fmaf(w.z, h.z, fmaf(w.w, h.w, s))));
+      }
+      s = fmaxf(s, 0.f);
+      A3[t * kS + o] = s;
+      y = fmaf(sp[oW4 + o], s, y);
+    }
+    const float err = valid ? y - T[i] : 0.f;
+    const float dy = err / (float)n;
+    lsum += 0.5f * err * err / (float)n;
+    DY[t] = dy;
+#pragma unroll 8
+    for (int o = 0; o < kH; o++) D3[t * kS + o] = A3[t * kS + o] > 0.f ? dy * sp[oW4 + o] : 0.f;
+    __syncthreads();
+
+    // ---- W3 (tile), W4, b3, b4 ----
+#pragma unroll 2
+    for (int b = 0; b < kMB; b++) {
+      const float4 d = ld4(D3 + b * kS + o0);
+      const float4 h0 = ld4(A2 + b * kS + k0), h1 = ld4(A2 + b * kS + k0 + 4);
+      const float dv[4] = {d.x, d.y, d.z, d.w};
+      const float hv[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) gW3[r][c] = fmaf(dv[r], hv[c], gW3[r][c]);
+    }
+    if (t < kH) {
+      for (int b = 0; b < kMB; b++) {
+        gW4 = fmaf(DY[b], A3[b * kS + t], gW4);
+        gB3 += D3[b * kS + t];
+      }
+    } else if (t == kH) {
+      for (int b = 0; b < kMB; b++) gB4 += DY[b];
+    }
+    // ---- delta 2 of this thread's sample: (W3^T d3) * relu'(a2) ----
+    float d2[kH];
+#pragma unroll
+    for (int k = 0; k < kH; k++) d2[k] = 0.f;
+#pragma unroll 2
+    for (int o = 0; o < kH; o++) {
+      const float d = D3[t * kS + o];
+#pragma unroll
+      for (int k = 0; k < kH; k += 4) {
+        const float4 w = ld4(sp + oW3 + o * kH + k);
+        d2[k] = fmaf(w.x, d, d2[k]);
+        d2[k + 1] = fmaf(w.y, d, d2[k + 1]);
+        d2[k + 2] = fmaf(w.z, d, d2[k + 2]);
+        d2[k + 3] = fmaf(w.w, d, d2[k + 3]);
+      }
+    }
+    __syncthreads();  // A3 and D3 are read by every thread above
+    float *D2 = A3;
+#pragma unroll
+    for (int k = 0; k < kH; k += 4) {
+      const float4 a = ld4(A2 + t * kS + k);
+      *reinterpret_cast<float4 *>(D2 + t * kS + k) =
+          make_float4(a.x > 0.f ? d2[k] : 0.f, a.y > 0.f ? d2[k + 1] : 0.f,
+                      a.z > 0.f ? d2[k + 2] : 0.f, a.w > 0.f ? d2[k + 3] : 0.f);
+    }
+    __syncthreads();
+
+    // ---- W2 (tile), b2 ----
+#pragma unroll 2
+    for (int b = 0; b < kMB; b++) {
+      const float4 d = ld4(D2 + b * kS + o0);
+      const float4 h0 = ld4(A1 + b * kS + k0), h1 = ld4(A1 + b * kS + k0 + 4);
+      const float dv[4] = {d.x, d.y, d.z, d.w};
+      const float hv[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) gW2[r][c] = fmaf(dv[r], hv[c], gW2[r][c]);
+    }
+    if (t < kH)
+      for (int b = 0; b < kMB; b++) gB2 += D2[b * kS + t];
+    // ---- delta 1 of this thread's sample: (W2^T d2) * relu'(a1) ----
+    float d1[kH];
+#pragma unroll
+    for (int k = 0; k < kH; k++) d1[k] = 0.f;
+#pragma unroll 2
+    for (int o = 0; o < kH; o++) {
+      const float d = D2[t * kS + o];
+#pragma unroll
+      for (int k = 0; k < kH; k += 4) {
+        const float4 w = ld4(sp + oW2 + o * kH + k);
+        d1[k] = fmaf(w.x, d, d1[k]);
+        d1[k + 1] = fmaf(w.y, d, d1[k + 1]);
+        d1[k + 2] = fmaf(w.z, d, d1[k + 2]);
+        d1[k + 3] = fmaf(w.w, d, d1[k + 3]);
+      }
+    }
+    float *D1 = D3;  // D3 is no longer read: every thread passed the barrier above
+#pragma unroll
+    for (int k = 0; k < kH; k += 4) {
+      const float4 a = ld4(A1 + t * kS + k);
+      *reinterpret_cast<float4 *>(D1 + t * kS + k) =
+          make_float4(a.x > 0.f ? d1[k] : 0.f, a.y > 0.f ? d1[k + 1] : 0.f,
+                      a.z > 0.f ? d1[k + 2] : 0.f, a.w > 0.f ? d1[k + 3] : 0.f);
+    }
+    __syncthreads();
+
+    // ---- W1, b1 (row t) ----
+    if (t < kH) {
+      for (int b = 0; b < kMB; b++) {
+        const float d = D1[b * kS + t];
+        gB1 += d;
+#pragma unroll
+        for (int k = 0; k < kIn; k++) gW1[k] = fmaf(d, XS[b * 8 + k], gW1[k]);
+      }
+    }
+    __syncthreads();  // the next chunk overwrites every array
   }
-  DY[tid] = dy;
-  __syncthreads();
-  // ---- layer 4: W4, b4 ----
-  if (tid < kH) {
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s = fmaf(DY[b], H3[tid * kMB + b], s);
-    atomicAdd(G + oW4 + tid, s);
+
+  // ---- one atomic per parameter per block ----
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      atomicAdd(G + oW3 + (o0 + r) * kH + k0 + c, gW3[r][c]);
+      atomicAdd(G + oW2 + (o0 + r) * kH + k0 + c, gW2[r][c]);
+    }
+  if (t < kH) {
+#pragma unroll
+    for (int k = 0; k < kIn; k++) atomicAdd(G + oW1 + t * kIn + k, gW1[k]);
+    atomicAdd(G + oB1 + t, gB1);
+    atomicAdd(G + oB2 + t, gB2);
+    atomicAdd(G + oB3 + t, gB3);
+    atomicAdd(G + oW4 + t, gW4);
+  } else if (t == kH) {
+    atomicAdd(G + oB4, gB4);
   }
-  if (tid == kH) {
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s += DY[b];
-    atomicAdd(G + oB4, s);
-  }
-  // ---- layer 3: W3[o][k] += sum_b D3[o][b] H2[k][b], b3 ----
-  for (int q = tid; q < kH * kH; q += kMB) {
-    const int o = q / kH, k = q % kH;
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s = fmaf(D3[o * kMB + b], H2[k * kMB + b], s);
-    atomicAdd(G + oW3 + q, s);
-  }
-  if (tid < kH) {
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s += D3[tid * kMB + b];
-    atomicAdd(G + oB3 + tid, s);
-  }
-  // delta of layer 2 for this thread's sample: (W3^T d3) * relu'(h2)
-  float d2[kH];
-  for (int k = 0; k < kH; k++) {
-    float s = 0.f;
-    for (int o = 0; o < kH; o++) s = fmaf(sp[oW3 + o * kH + k], D3[o * kMB + tid], s);
-    d2[k] = h2[k] > 0.f ? s : 0.f;
-  }
-  __syncthreads();  // everyone is done reading H3 / D3
-  float *D2 = H3;
-  for (int k = 0; k < kH; k++) D2[k * kMB + tid] = d2[k];
-  __syncthreads();
-  // ---- layer 2 ----
-  for (int q = tid; q < kH * kH; q += kMB) {
-    const int o = q / kH, k = q % kH;
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s = fmaf(D2[o * kMB + b], H1[k * kMB + b], s);
-    atomicAdd(G + oW2 + q, s);
-  }
-  if (tid < kH) {
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s += D2[tid * kMB + b];
-    atomicAdd(G + oB2 + tid, s);
-  }
-  float d1[kH];
-  for (int k = 0; k < kH; k++) {
-    float s = 0.f;
-    for (int o = 0; o < kH; o++) s = fmaf(sp[oW2 + o * kH + k], D2[o * kMB + tid], s);
-    d1[k] = h1[k] > 0.f ? s : 0.f;
-  }
-  __syncthreads();
-  float *D1 = D3;
-  for (int k = 0; k < kH; k++) D1[k * kMB + tid] = d1[k];
-  __syncthreads();
-  // ---- layer 1 ----
-  for (int q = tid; q < kH * kIn; q += kMB) {
-    const int o = q / kIn, k = q % kIn;
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s = fmaf(D1[o * kMB + b], XS[k * kMB + b], s);
-    atomicAdd(G + oW1 + q, s);
-  }
-  if (tid < kH) {
-    float s = 0.f;
-    for (int b = 0; b < kMB; b++) s += D1[tid * kMB + b];
-    atomicAdd(G + oB1 + tid, s);
-  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
+  if (lane == 0) atomicAdd(loss, lsum);
 }
 
 // Adam step (bias-corrected) on all parameters.
@@ -198,7 +312,7 @@ __global__ void mlp_adam_kernel(float *P, const float *G, float *M, float *V, in
   P[k] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
 }
 
-constexpr size_t kBwdSmem = sizeof(float) * (kNP + kIn * kMB + 4 * kH * kMB + kMB);
+constexpr size_t kBwdSmem = sizeof(float) * kBwdFloats;
 
 uint64_t splitmix(uint64_t &s) {
   uint64_t z = (s += 0x9E3779B97F4A7C15ull);
@@ -223,6 +337,13 @@ struct sapb_mlp {
     if (e_ != cudaSuccess)                                                                 \
       return sapb_fail((m)->d, SAPB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));       \
   } while (0)
+
+// persistent backward grid: one block per SM at most (its shared memory
+// allows one), never more blocks than chunks of 128 samples
+static int bwd_grid(const sapb_mlp *m, int n) {
+  const int chunks = (n + kMB - 1) / kMB;
+  return std::max(1, std::min(chunks, m->d->num_sms));
+}
 
 static int mlp_reserve(sapb_mlp *m, int n) {
   if (n <= m->cap) return SAPB_OK;
@@ -342,7 +463,7 @@ int sapb_mlp_gradient(sapb_mlp *m, int n, const float *x, const float *t, float 
   MK(m, cudaMemcpyAsync(m->T, t, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
   MK(m, cudaMemsetAsync(m->G, 0, sizeof(float) * kNP, st));
   MK(m, cudaMemsetAsync(m->loss, 0, sizeof(float), st));
-  mlp_backward_kernel<<<(n + kMB - 1) / kMB, kMB, kBwdSmem, st>>>(m->P, n, m->X, m->T, m->G,
+  mlp_backward_kernel<<<bwd_grid(m, n), kMB, kBwdSmem, st>>>(m->P, n, m->X, m->T, m->G,
                                                                  m->loss);
   MK(m, cudaGetLastError());
   if (grad) MK(m, cudaMemcpyAsync(grad, m->G, sizeof(float) * kNP, cudaMemcpyDeviceToHost, st));
@@ -365,7 +486,7 @@ int sapb_mlp_train(sapb_mlp *m, int n, const float *x, const float *t, int epoch
   for (int e = 0; e < epochs; e++) {
     MK(m, cudaMemsetAsync(m->G, 0, sizeof(float) * kNP, st));
     MK(m, cudaMemsetAsync(m->loss, 0, sizeof(float), st));
-    mlp_backward_kernel<<<(n + kMB - 1) / kMB, kMB, kBwdSmem, st>>>(m->P, n, m->X, m->T, m->G,
+    mlp_backward_kernel<<<bwd_grid(m, n), kMB, kBwdSmem, st>>>(m->P, n, m->X, m->T, m->G,
                                                                    m->loss);
     m->steps++;
     const float b1 = 0.9f, b2 = 0.999f;
