@@ -114,6 +114,9 @@ _SIGS = [
     ("sapb_mlp_gradient", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float), C.POINTER(C.c_float),
                                     C.POINTER(C.c_float)]),
+    ("sapb_mlp_propose", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
+                                   C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float)]),
     ("sapb_mlp_train", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                  C.c_int, C.c_float, C.POINTER(C.c_float)]),
     # class binding

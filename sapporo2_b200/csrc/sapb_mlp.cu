@@ -76,6 +76,42 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(const float *__restric
   Y[i] = mlp_eval(sp, x, nullptr, nullptr, nullptr);
 }
 
+// Proposal: the five features of each particle from its raw previous state
+// (n_prev, h2_prev, a[3], jerk[3]; logarithms of the density estimate
+// n / (4/3 pi h^3), |a|, |jerk|, 1 + n, h2 with n = max(n_prev, 1/2)),
+// standardised with (mu, sd), the network's correction clipped to
+// [-max_down, max_up] and added to the count-scaled step 2/3 log(target/n);
+// out: h2_prev * exp(clip(step, -clip, clip)).
+struct MlpScale {
+  float mu[kIn], sd[kIn];
+  float target, max_down, max_up, clip;
+};
+constexpr int kPropIn = 8;
+
+__global__ void __launch_bounds__(128) mlp_propose_kernel(const float *__restrict__ P, int n,
+                                                          const float *__restrict__ IN,
+                                                          MlpScale sc, float *__restrict__ H2) {
+  __shared__ float sp[kNP];
+  for (int k = threadIdx.x; k < kNP; k += blockDim.x) sp[k] = P[k];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float *r = IN + (size_t)i * kPropIn;
+  const float np = fmaxf(r[0], 0.5f), h2 = r[1];
+  const float an = sqrtf(r[2] * r[2] + r[3] * r[3] + r[4] * r[4]) + 1e-30f;
+  const float jn = sqrtf(r[5] * r[5] + r[6] * r[6] + r[7] * r[7]) + 1e-30f;
+  const float lh2 = logf(h2);
+  const float f[kIn] = {logf(np) - logf(4.18879020f) - 1.5f * lh2, logf(an), logf(jn),
+                        log1pf(np), lh2};
+  float x[kIn];
+#pragma unroll
+  for (int k = 0; k < kIn; k++) x[k] = (f[k] - sc.mu[k]) / sc.sd[k];
+  const float corr = fminf(fmaxf(mlp_eval(sp, x, nullptr, nullptr, nullptr), -sc.max_down),
+                           sc.max_up);
+  const float step = (2.f / 3.f) * logf(sc.target / np) + corr;
+  H2[i] = h2 * expf(fminf(fmaxf(step, -sc.clip), sc.clip));
+}
+
 // Gradient of L = 1/(2n) sum (y - t)^2 over the n samples, accumulated into
 // G (zeroed by the caller), loss accumulated into *loss.
 //
@@ -353,7 +389,7 @@ static int mlp_reserve(sapb_mlp *m, int n) {
   cudaFree(m->Y);
   m->X = m->T = m->Y = nullptr;
   m->cap = 0;
-  if (cudaMalloc(&m->X, sizeof(float) * kIn * (size_t)cap) != cudaSuccess ||
+  if (cudaMalloc(&m->X, sizeof(float) * kPropIn * (size_t)cap) != cudaSuccess ||
       cudaMalloc(&m->T, sizeof(float) * (size_t)cap) != cudaSuccess ||
       cudaMalloc(&m->Y, sizeof(float) * (size_t)cap) != cudaSuccess) {
     cudaGetLastError();
@@ -448,6 +484,32 @@ int sapb_mlp_forward(sapb_mlp *m, int n, const float *x, float *y) {
   mlp_forward_kernel<<<(n + 127) / 128, 128, 0, st>>>(m->P, n, m->X, m->Y);
   MK(m, cudaGetLastError());
   MK(m, cudaMemcpyAsync(y, m->Y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
+  MK(m, cudaStreamSynchronize(st));
+  return SAPB_OK;
+}
+
+int sapb_mlp_propose(sapb_mlp *m, int n, const float *in, const float *mu, const float *sd,
+                     float target, float max_down, float max_up, float clip, float *h2_out) {
+  if (!m || n < 0 || (n && (!in || !mu || !sd || !h2_out)) || !(target > 0.f))
+    return sapb_fail(m ? m->d : nullptr, SAPB_EINVAL, "bad arguments");
+  if (n == 0) return SAPB_OK;
+  MK(m, cudaSetDevice(m->d->device));
+  int rc = mlp_reserve(m, n);
+  if (rc) return rc;
+  MlpScale sc;
+  for (int k = 0; k < kIn; k++) {
+    sc.mu[k] = mu[k];
+    sc.sd[k] = sd[k];
+  }
+  sc.target = target;
+  sc.max_down = max_down;
+  sc.max_up = max_up;
+  sc.clip = clip;
+  cudaStream_t st = m->d->stream;
+  MK(m, cudaMemcpyAsync(m->X, in, sizeof(float) * kPropIn * (size_t)n, cudaMemcpyHostToDevice, st));
+  mlp_propose_kernel<<<(n + 127) / 128, 128, 0, st>>>(m->P, n, m->X, sc, m->Y);
+  MK(m, cudaGetLastError());
+  MK(m, cudaMemcpyAsync(h2_out, m->Y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
   MK(m, cudaStreamSynchronize(st));
   return SAPB_OK;
 }

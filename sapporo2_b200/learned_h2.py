@@ -137,7 +137,29 @@ class H2Net:
     def propose(self, n_prev, h2_prev, acc, jrk, clip=4.0) -> np.ndarray:
         """h2 for the next evaluation: the count-scaled radius times the
         network's bounded correction; the whole log-ratio is clipped to
-        +-clip."""
+        +-clip.  Features, standardisation, network and correction run in
+        one kernel (sapb_mlp_propose) from the raw per-particle state."""
+        if self.mu is None:
+            self.fit_standardisation(features(n_prev, h2_prev, acc, jrk))
+        n = len(h2_prev)
+        rec = np.empty((n, 8), dtype=np.float32)
+        rec[:, 0] = n_prev
+        rec[:, 1] = h2_prev
+        rec[:, 2:5] = acc
+        rec[:, 5:8] = jrk
+        mu = self._f(self.mu)
+        sd = self._f(self.sd)
+        out = np.empty(n, dtype=np.float32)
+        fp = C.POINTER(C.c_float)
+        _check(self.lib.sapb_mlp_propose(self.h, n, rec.ctypes.data_as(fp), mu.ctypes.data_as(fp),
+                                         sd.ctypes.data_as(fp), float(TARGET),
+                                         float(self.MAX_DOWN), float(self.MAX_UP), float(clip),
+                                         out.ctypes.data_as(fp)), "mlp_propose", self.owner.dev)
+        return out.astype(np.float64)
+
+    def propose_host(self, n_prev, h2_prev, acc, jrk, clip=4.0) -> np.ndarray:
+        """The same proposal with the features built on the host (FP64) and
+        only the network on the GPU -- the reference for propose()."""
         f = self.standardise(features(n_prev, h2_prev, acc, jrk))
         corr = np.clip(self.forward(f).astype(np.float64), -self.MAX_DOWN, self.MAX_UP)
         r = self.base_log_ratio(n_prev) + corr

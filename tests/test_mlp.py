@@ -71,3 +71,23 @@ def test_gpu_training_fits_a_smooth_target(gpu):
         l1 = M.loss(net.params().astype(np.float64), x, t)
         net.close()
     assert l1 < 0.02 * l0, (l0, l1)
+
+
+@gpu
+def test_gpu_proposal_kernel_matches_the_host_features(gpu):
+    """sapb_mlp_propose (features, standardisation, network, bounded
+    correction in one kernel) against features built on the host."""
+    import sapporo2_b200 as sp
+    from sapporo2_b200.learned_h2 import H2Net
+    rng = np.random.default_rng(8)
+    n = 3000
+    n_prev = rng.integers(0, 300, n).astype(np.float64)
+    h2 = 10.0 ** rng.uniform(-6, -1, n)
+    acc = rng.normal(size=(n, 3)) * 10.0 ** rng.uniform(-2, 2, (n, 1))
+    jrk = rng.normal(size=(n, 3)) * 10.0 ** rng.uniform(-1, 3, (n, 1))
+    with sp.Sapporo(order=sp.SIXTH) as s:
+        net = H2Net(s, seed=13)
+        want = net.propose_host(n_prev, h2, acc, jrk)
+        got = net.propose(n_prev, h2, acc, jrk)
+        net.close()
+    np.testing.assert_allclose(got, want, rtol=2e-5)
