@@ -10,7 +10,7 @@
 //     dsmin_i written only when taken (:722-775);
 //   - neighbour lists: overflow when a count reaches NGB_PB (:804-835),
 //     get_ngb_list copies and sorts (:837-880).
-// Deviations (documented in DESIGN.md): fatal exits become error returns;
+// Deviations: fatal exits become error returns;
 // one GPU is used whatever the device list says; get_ngb_list never copies
 // more than NGB_PB entries and flags overflow when the count reaches NGB_PB.
 #include "../../include/sapporohostclass.h"

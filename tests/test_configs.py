@@ -85,7 +85,7 @@ def test_c3_precision_form_2_20(gpu):
                           pv, pa, cfg["m"], cfg["id"], cfg["eps2"])
     sub = {f: got[f][sel] for f in ("acc", "jrk", "snp", "pot")}
     st = T.check_forces(sub, want, 2)
-    assert st["acc"][0] <= 1e-6  # north_star: median relative acc error vs FP64
+    assert st["acc"][0] <= 1e-6  # the required median relative acc error vs FP64
     print(st)
 
 
