@@ -138,7 +138,7 @@ int sapb_wait_selftest(sapb_dev *d, int limit_ms);
  * their own pool allocator, or that must not take the device-wide
  * synchronisation cudaFree implies in the middle of a time step -- whereas
  * sapb_force_device grows its partial-sum buffer with cudaMalloc/cudaFree
- * when a larger active set arrives.  This build-specific entry point has no
+ * when a larger active set arrives.  This entry point of this library has no
  * counterpart in the reference.
  *
  * Same arguments, layouts and results as sapb_force_device.  The j-split

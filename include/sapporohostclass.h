@@ -5,7 +5,7 @@
  * (lib/include/sapporohostclass.h:37-176): same class name, method names,
  * argument order and meaning, default arguments and enum values, so callers
  * written against the reference compile and link unchanged.  The private
- * part is this build's own (one GPU behind the sapb_* C ABI of
+ * part is this library's own (one GPU behind the sapb_* C ABI of
  * sapporo_b200.h); no binary layout compatibility is implied.
  *
  * Like the reference header it pulls in <iostream>, <vector>, <map>,
@@ -117,7 +117,7 @@ class sapporo {
   int read_ngb_list(int);
   int get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, int nbl[]);
 
-  // Additions of this build (not in the reference): the underlying device
+  // Additions of this library (not in the reference): the underlying device
   // handle, and the status of the last call that can fail (0 = ok).
   sapb_dev *device_handle() { return dev_; }
   int last_status;

@@ -348,7 +348,7 @@ int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "cudaGetDeviceProperties"); break; }
     d->num_sms = prop.multiProcessorCount;
     if (prop.major < 10) {
-      rc = fail(d, SAPB_ENODEV, "device %d is sm_%d%d; this build targets sm_100a", device,
+      rc = fail(d, SAPB_ENODEV, "device %d is sm_%d%d; this library targets sm_100a", device,
                 prop.major, prop.minor);
       break;
     }

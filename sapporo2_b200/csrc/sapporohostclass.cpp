@@ -67,7 +67,7 @@ int sapporo::open(std::string kernelFile, int *devices, int nprocs, int order, i
   int device = 0;
   if (nprocs > 0 && devices) device = devices[0];
   if (nprocs > 1 || nprocs < -1)
-    fprintf(stderr, "sapporo: %d devices requested; this build drives one GPU (device %d)\n",
+    fprintf(stderr, "sapporo: %d devices requested; this library drives one GPU (device %d)\n",
             nprocs < 0 ? -nprocs : nprocs, device);
   const char *np = getenv("SAPPORO_NPIPES");
   const int pipes = np ? atoi(np) : NPIPES;
