@@ -93,6 +93,14 @@ static int grow_j(sapb_dev *d, int new_cap) {
   int *id = nullptr;
   void *pred = nullptr;
   const size_t pb = pred_bytes_per_j(d->order, d->prec);
+  {  // refuse up front what cannot fit (no attempt, no partial allocation)
+    const size_t need = ((size_t)np * 8 + 4 + pb) * (size_t)new_cap;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need > free_b)
+      return fail(d, SAPB_ENOMEM,
+                  "cannot allocate j storage for %d particles: %.1f GB needed, %.1f GB free",
+                  new_cap, need / 1e9, free_b / 1e9);
+  }
   if (cudaMalloc(&pool, sizeof(double) * np * (size_t)new_cap) != cudaSuccess ||
       cudaMalloc(&id, sizeof(int) * (size_t)new_cap) != cudaSuccess ||
       cudaMalloc(&pred, pb * (size_t)new_cap) != cudaSuccess) {
