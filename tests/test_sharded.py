@@ -149,3 +149,45 @@ def test_sharded_single_rank_on_gpu_equals_the_class(gpu):
         assert a[0] == b[0] and a[1] == b[1]
         if b[1] < NGB_PB:  # which 256 ids an overflowing list keeps is not defined
             np.testing.assert_array_equal(a[2], b[2])
+
+
+def _integrate_rank(rank, world, port, out):
+    import torch.distributed as dist
+
+    from sapporo2_b200 import hermite6 as H
+    from sapporo2_b200.sharded import ShardedSapporo
+    from tests.oracle_backend import OracleBackend
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    cfg = ic.make_config("C5", n=768, seed=9)
+    sim = H.BlockHermite6(cfg["x"], cfg["v"], cfg["m"], cfg["eps2"], H.CountScaledH2(),
+                          backend=ShardedSapporo(OracleBackend(768, lists=True)))
+    for _ in range(8):
+        sim.step()
+    if rank == 0:
+        np.savez(out, x=sim.x, v=sim.v, t=sim.t, cnt=sim.n_prev)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_block_step_integrator_on_two_gloo_ranks():
+    """The 6th-order block-step driver with its j split over two ranks takes
+    the same steps as with one oracle holding every j."""
+    import torch.multiprocessing as mp
+
+    from sapporo2_b200 import hermite6 as H
+    from tests.oracle_backend import OracleBackend
+    cfg = ic.make_config("C5", n=768, seed=9)
+    sim = H.BlockHermite6(cfg["x"], cfg["v"], cfg["m"], cfg["eps2"], H.CountScaledH2(),
+                          backend=OracleBackend(768, lists=True))
+    for _ in range(8):
+        sim.step()
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "r0.npz")
+        mp.start_processes(_integrate_rank, args=(2, _free_port(), out), nprocs=2, join=True,
+                           start_method="spawn")
+        got = np.load(out)
+        np.testing.assert_array_equal(got["t"], sim.t)
+        np.testing.assert_allclose(got["x"], sim.x, rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(got["v"], sim.v, rtol=1e-10, atol=1e-12)
+        np.testing.assert_array_equal(got["cnt"], sim.n_prev)
