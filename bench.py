@@ -401,6 +401,74 @@ def run_learned_h2_bench(args):
     }), flush=True)
 
 
+def run_blocksteps_bench(args):
+    """Block time steps of one system (N = 131072 Plummer, 6th order,
+    dt = 2^-k with k uniform in 3..12, lists on with h2 for ~32 neighbours):
+    the first `bs_steps` block times of the 2^-12 grid, each with the active
+    set its block-bin occupancy gives.  Per step the active particles' j
+    records are re-staged, then the force on the active set is computed
+    (a) through the sapporo class (set_time, startGravCalc, getGravResults)
+    and (b) through the batch API (plan, i records, one graph replay,
+    results).  Host wall time per step, i records prepared beforehand."""
+    import sapporo2_b200 as sp
+    from sapporo2_b200 import ic
+    from sapporo2_b200.direct import fp64_direct
+    cfg = ic.make_config("C2")
+    n, k = cfg["n"], cfg["k"]
+    x, v, m, ids, eps2 = cfg["x"], cfg["v"], cfg["m"], cfg["id"], cfg["eps2"]
+    a, j, _ = fp64_direct(1, x, v, None, m, ids, eps2)
+    _, _, sn = fp64_direct(2, x, v, a, m, ids, eps2)
+    c = ic.crackle_from(x, a, j)
+    steps = []
+    for st in range(1, args.bs_steps + 1):
+        T_, t0, act = ic.block_state(k, st)
+        px, pv, pa = ic.predict_fp64(2, T_, t0[act], x[act], v[act], a[act], j[act], sn[act],
+                                     c[act])
+        steps.append((T_, t0, act, px, pv, pa))
+    inter = float(sum(len(q[2]) for q in steps)) * n
+    out = {}
+    with sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE, n_pipes=n) as s:
+        s.set_j_particles(np.arange(n), ids, np.zeros(n), m, x, v, a, j, sn, c)
+        for mode in ("class", "batch", "class", "batch"):  # second pass timed
+            times = []
+            b = sp.Batch(s, 1, n) if mode == "batch" else None
+            for T_, t0, act, px, pv, pa in steps:
+                t_a = time.perf_counter()
+                s.set_j_particles(act, ids[act], t0[act], m[act], x[act], v[act], a[act],
+                                  j[act], sn[act], c[act])
+                if mode == "class":
+                    s.set_time(T_)
+                    s.start(n, ids[act], px, pv, pa, eps2, cfg["h2"][act])
+                    r = s.results(n)
+                else:
+                    s.set_no_time()  # the batch run predicts; here only the upload
+                    s.force_prediction(n)
+                    b.plan([0], [n], [len(act)], [T_], [eps2])
+                    b.i_stage[:len(act)] = sp.pack_i_records(2, px, pv, cfg["h2"][act],
+                                                             ids[act], pa)
+                    b.run(sp.F_PREDICT | sp.F_NGB_LIST)
+                    r = b.results()
+                times.append(time.perf_counter() - t_a)
+            if b is not None:
+                b.close()
+            out[mode] = {"s_total": float(np.sum(times)),
+                         "ms_per_step": 1e3 * float(np.mean(times)),
+                         "interactions_per_s": inter / float(np.sum(times))}
+    act_n = np.array([len(q[2]) for q in steps])
+    print(json.dumps({
+        "metric": "interactions/s over block steps (N=131072 Plummer, 6th order, dt=2^-k, "
+                  "k in 3..12, lists on), host wall time per step",
+        "value": out["class"]["interactions_per_s"], "unit": "interactions/s", "n_gpus": 1,
+        "steps": args.bs_steps, "warmup": args.bs_steps, "ms_per_step": out["class"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 body + ds positions + f64 sums", "data": "synthetic",
+        "config": {"workload": "block steps of one system (C2)", "n": n,
+                   "block_steps": args.bs_steps, "active_mean": float(act_n.mean()),
+                   "active_min": int(act_n.min()), "active_max": int(act_n.max()),
+                   "class_api": out["class"], "batch_api": out["batch"]},
+    }), flush=True)
+
+
 def rel_stats(got, want):
     e = np.linalg.norm(got - want, axis=1) / np.maximum(np.linalg.norm(want, axis=1), 1e-300)
     return {"median": float(np.median(e)), "max": float(e.max())}
@@ -461,10 +529,12 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2"],
+    ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2", "blocksteps"],
                     default="precision",
                     help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters; "
-                         "learned_h2: block steps with fixed, count-scaled and learned h2")
+                         "learned_h2: block steps with fixed, count-scaled and learned h2; "
+                         "blocksteps: block steps of one system, class vs batch API")
+    ap.add_argument("--bs-steps", type=int, default=64)
     ap.add_argument("--multi", choices=["shard", "replicas"], default="shard",
                     help="N>1 GPUs: shard: one N-body system, j split over the ranks "
                          "(strong scaling); replicas: an independent system per rank")
@@ -504,6 +574,9 @@ def main():
         return
     if args.workload == "learned_h2":
         run_learned_h2_bench(args)
+        return
+    if args.workload == "blocksteps":
+        run_blocksteps_bench(args)
         return
     n = args.n
     sharded = world > 1 and args.multi == "shard"
