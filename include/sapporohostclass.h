@@ -118,9 +118,16 @@ class sapporo {
   int get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, int nbl[]);
 
   // Additions of this library (not in the reference): the underlying device
-  // handle, and the status of the last call that can fail (0 = ok).
+  // handle, the status of the last call that can fail (0 = ok), and n calls
+  // of set_j_particle in one (arrays of n, vectors [n][3]; a, jrk, snp, crk,
+  // eps, t may be null for zeros): the same address rules, one staging
+  // reservation for all.
   sapb_dev *device_handle() { return dev_; }
   int last_status;
+  int set_j_particles(int n, const int *address, const int *id, const double *t,
+                      const double *mass, const double *x, const double *v, const double *a,
+                      const double *jrk, const double *snp, const double *crk,
+                      const double *eps);
 };
 
 #endif

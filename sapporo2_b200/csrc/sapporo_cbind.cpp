@@ -35,16 +35,7 @@ int sapporo_c_set_j_particles(sapporo_c *s, int n, const int *address, const int
                               const double *v, const double *a, const double *jrk,
                               const double *snp, const double *crk, const double *eps) {
   if (!s || n < 0) return SAPB_EINVAL;
-  double k18[3] = {0, 0, 0};
-  for (int k = 0; k < n; k++) {
-    const int rc = s->obj.set_j_particle(
-        address[k], id[k], t ? t[k] : 0.0, 0.0, mass[k], k18, const_cast<double *>(jrk + 3 * k),
-        const_cast<double *>(a + 3 * k), const_cast<double *>(v + 3 * k),
-        const_cast<double *>(x + 3 * k), snp ? const_cast<double *>(snp + 3 * k) : nullptr,
-        crk ? const_cast<double *>(crk + 3 * k) : nullptr, eps ? eps[k] : 0.0);
-    if (rc) return rc;
-  }
-  return 0;
+  return s->obj.set_j_particles(n, address, id, t, mass, x, v, a, jrk, snp, crk, eps);
 }
 
 int sapporo_c_start(sapporo_c *s, int nj, int ni, const int *id, const double *xi,

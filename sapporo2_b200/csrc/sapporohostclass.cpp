@@ -18,6 +18,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/sapporo_b200.h"
 
@@ -182,6 +183,73 @@ int sapporo::set_j_particle(int address, int id, double tj, double dtj, double m
       r[16 + d] = snp ? snp[d] : 0.0;
       r[19 + d] = crk ? crk[d] : 0.0;
     }
+  }
+  return 0;
+}
+
+int sapporo::set_j_particles(int n, const int *address, const int *id, const double *t,
+                             const double *mass, const double *x, const double *v,
+                             const double *a, const double *jrk, const double *snp,
+                             const double *crk, const double *eps) {
+  if (!dev_ || n < 0 || (n && (!address || !id || !mass || !x))) return last_status = SAPB_EINVAL;
+  if (n == 0) return 0;
+  // the address rules of set_j_particle, in the given order; on a bad address
+  // nothing of this call is staged
+  for (int k = 0; k < n; k++) {
+    const int addr = address[k];
+    if (addr < 0) {
+      fprintf(stderr, "sapporo::set_j_particles: negative address %d\n", addr);
+      return last_status = SAPB_EINVAL;
+    }
+    if (addr >= nj_max) {
+      increase_jMemory();
+      if (addr >= nj_max) {
+        fprintf(stderr,
+                "sapporo::set_j_particles: address %d beyond %d after growing; send particles "
+                "in address order\n",
+                addr, nj_max);
+        return last_status = SAPB_EINVAL;
+      }
+    }
+  }
+  predJOnHost = false;
+  nj_updated = true;
+  // slots, then one staging reservation and a tight fill
+  std::vector<int> slots((size_t)n);
+  for (int k = 0; k < n; k++) {
+    const int addr = address[k];
+    int slot = stage_slot_[addr];
+    if (slot < 0) {
+      slot = nstaged_++;
+      stage_slot_[addr] = slot;
+      staged_addr_.push_back(addr);
+    }
+    slots[k] = slot;
+  }
+  double *base = sapb_j_stage(dev_, nstaged_);
+  if (!base) {
+    report("j staging", SAPB_ENOMEM, dev_);
+    return last_status = SAPB_ENOMEM;
+  }
+  const int ss = sapb_j_stage_stride(dev_);
+  const bool six = integrationOrder > FOURTH;
+  for (int k = 0; k < n; k++) {
+    double *r = base + (size_t)slots[k] * ss;
+    put_int_pair(&r[0], address[k], id[k]);
+    r[1] = t ? t[k] : 0.0;
+    r[2] = mass[k];
+    for (int d = 0; d < 3; d++) {
+      r[3 + d] = x[3 * k + d];
+      r[6 + d] = v ? v[3 * k + d] : 0.0;
+      r[9 + d] = a ? a[3 * k + d] : 0.0;
+      r[12 + d] = jrk ? jrk[3 * k + d] : 0.0;
+    }
+    r[15] = eps ? eps[k] : 0.0;
+    if (six)
+      for (int d = 0; d < 3; d++) {
+        r[16 + d] = snp ? snp[3 * k + d] : 0.0;
+        r[19 + d] = crk ? crk[3 * k + d] : 0.0;
+      }
   }
   return 0;
 }
