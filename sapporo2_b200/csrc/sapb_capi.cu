@@ -154,6 +154,7 @@ static int ensure_i(sapb_dev *d, int ni) {
     if (lst) cudaFree(lst);
     return fail(d, SAPB_ENOMEM, "cannot allocate i buffers for %d particles", cap);
   }
+  cudaStreamSynchronize(d->stream);  // a call in flight may still use the old buffers
   if (d->irec_h) {
     memcpy(ih, d->irec_h, sizeof(double) * is * (size_t)d->i_cap);
     cudaFreeHost(d->irec_h);
@@ -189,9 +190,8 @@ static int ensure_part(sapb_dev *d, size_t doubles) {
 }
 
 // ---------------------------------------------------------------------
-// Launch planner: threads-per-i, i per thread and the number of j slices.
-// Scores every shape by the fraction of i slots that carry a particle
-// times how well the grid fills `target` resident blocks.
+// Launch planner: threads-per-i, i per thread and the number of j slices
+// (cost model in make_plan below).
 // ---------------------------------------------------------------------
 struct Plan {
   int tpi, ip, ns, i_tiles, slice_tiles;
