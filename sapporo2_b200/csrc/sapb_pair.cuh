@@ -59,7 +59,7 @@ __device__ __forceinline__ void taylor(const JState &js, int k, double ti, doubl
 }
 
 constexpr int kBT = 128;
-constexpr int kTJ = 128;
+constexpr int kTJ = 256;
 constexpr int kNS = 3;
 
 template <int ORDER, int PREC, int TPI, int IP>
