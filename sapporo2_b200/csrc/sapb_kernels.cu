@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti,
 // Block = 4 warps, laid out as TPI rows x TIT = 128/TPI columns; each thread
 // owns IP i-particles (columns tx, tx+TIT, ...), so a block covers an i-tile
 // of TI = TIT*IP particles.  blockIdx.y selects a j-slice of `slice_tiles`
-// tiles of TJ = 128 records.  Lane 0 of warp 0 streams the slice's tiles
+// tiles of kTJ = 256 records.  Lane 0 of warp 0 streams the slice's tiles
 // into a 3-stage shared-memory ring with cp.async.bulk (TMA engine): `full`
 // mbarriers signal arrival (complete_tx), `empty` mbarriers collect one
 // arrival per warp; there is no block-wide barrier per tile, so warps drift
