@@ -41,7 +41,7 @@ METRIC = "interactions/s at N=2^20 mixed vs plain FP64, 1 GPU, acc err<=1e-6; %F
 # DRAM bytes of one mixed 6th-order force launch at N = 2^20, all i, from
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (one pass) of
 # `bench.py --steps 1 --warmup 0 --only mixed --no-cpu`
-FORCE_DRAM_BYTES = 837.37e6 + 117.70e6
+FORCE_DRAM_BYTES = 968.47e6 + 182.86e6
 
 
 def log(*a):
@@ -683,7 +683,7 @@ def main():
                      "traffic": FORCE_DRAM_BYTES if (n == 1 << 20 and nj_loc == n) else None,
                      "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one "
                                      "force_kernel<6th,DS> launch at N=2^20 (ncu, 1 pass): "
-                                     "837.4 MB read + 117.7 MB written in 2.07 s, 0.46 GB/s; "
+                                     "968.5 MB read + 182.9 MB written in 2.03 s, 0.57 GB/s; "
                                      "j records stream from L2",
                      "peak_note": f"derived: {nsm} SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz "
                                   "(sm_max_mhz of measured peaks; no FP32 entry there)",

@@ -113,8 +113,7 @@ __global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti,
 // in FP32 (double-single difference, kernels.cu:169-177), FP32 body with
 // rsqrt on the MUFU pipe (two i per thread as packed FP32x2), FP32 sums per
 // tile folded into FP64 totals (shared memory) after every tile.
-// FP64 (DOUBLE): every step in double; 1/sqrt by Newton-Raphson from the MUFU
-// seed (rsqrt_nr64).
+// FP64 (DOUBLE): every step in double, rsqrt(double).
 //
 // The self pair (id_i == id_j, kernels.cu:565) is removed by replacing dx
 // with a huge value, which makes ds2 ~ 1e36 (1e300 in FP64): its force

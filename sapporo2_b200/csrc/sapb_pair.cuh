@@ -292,18 +292,6 @@ __device__ __forceinline__ double pair_dr_dp(const IDp &I, const double4 &r0, co
   return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
 }
 
-// rsqrt in FP64 for x in [FLT_MIN, FLT_MAX]: a 23-bit seed from the MUFU
-// (rsqrt.approx.ftz.f32 of x rounded to float) and two Newton-Raphson steps
-// y <- y (3/2 - x/2 y^2) in FP64 (quadratic convergence: 2^-22 -> 2^-44 ->
-// below 1 ulp before rounding).  x = +inf (the masked self pair) gives 0.
-__device__ __forceinline__ double rsqrt_nr64(double x) {
-  double y = (double)rsqrt_mufu(__double2float_rn(x));
-  const double hx = 0.5 * x;
-  y = y * fma(-hx, y * y, 1.5);
-  y = y * fma(-hx, y * y, 1.5);
-  return y;
-}
-
 // Same algebra as pair_mix: a3 = -3 alpha, b3 = -3 beta,
 //   jerk_ij = minv3 t,  t = dv + a3 dr
 //   snap_ij = minv3 (da + b3 dr + 2 a3 t)      (kernels.cu:642-667)
@@ -313,7 +301,7 @@ __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const d
   double dx, dy, dz;
   const double ds2 = pair_dr_dp(I, r0, r1, dx, dy, dz);
   tmin = fmin(tmin, ds2);
-  const double inv = rsqrt_nr64(ds2 + eps2);
+  const double inv = rsqrt(ds2 + eps2);
   const double inv2 = inv * inv;
   const double minv = r0.w * inv;
   const double minv3 = minv * inv2;

@@ -79,8 +79,8 @@ def test_small_active_sets(gpu, ni):
 
 @pytest.mark.parametrize("eps2", [0.0, 1e-6])
 def test_fp64_kernel_rsqrt_over_scales(gpu, eps2):
-    """The FP64 kernels take 1/sqrt by Newton-Raphson from a MUFU seed: one j
-    at the origin, i at distances 1e-6 .. 1e2, against long-double sums."""
+    """1/sqrt in the FP64 kernels over eight decades of distance: one j at
+    the origin, i at distances 1e-6 .. 1e2, against long-double sums."""
     rng = np.random.default_rng(17)
     n_i = 2000
     d = 10.0 ** rng.uniform(-6, 2, n_i)
