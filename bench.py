@@ -193,10 +193,17 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
             comb_ms.append(e2.elapsed_time(e3))
     stream.synchronize()
     out = res.cpu().numpy()
+    far_tiles, warp_tiles = s.spatial_stats(reset=True)
     s.close()
+    spatial = precision == sp.DOUBLESINGLE and spatial_on(n, nj)
+    # own kernels per step: predictor, force (+ slice reduction); in spatial
+    # mode the orderings add frame init, frame, j keys, gather, i keys and
+    # seeds (the two radix sorts are CUB's kernels, listed apart)
     return {"pred_ms": pred_ms, "force_ms": force_ms, "comb_ms": comb_ms, "res": out,
             "plan": {"tpi": tpi, "ip": ip, "nslices": ns}, "nj_local": nj,
-            "launches_per_step": 2 + (1 if ns > 1 else 0)}
+            "spatial": spatial,
+            "far_fraction": far_tiles / warp_tiles if warp_tiles else None,
+            "launches_per_step": 2 + (1 if ns > 1 else 0) + (6 if spatial else 0)}
 
 
 def e2e_arm(cfg, steps: int, shard=None):
@@ -461,7 +468,7 @@ def run_blocksteps_bench(args):
         "value": out["class"]["interactions_per_s"], "unit": "interactions/s", "n_gpus": 1,
         "steps": args.bs_steps, "warmup": args.bs_steps, "ms_per_step": out["class"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 body + ds positions + f64 sums", "data": "synthetic",
+        "dtype": "f32 body + ds positions (near tiles) + f64 sums", "data": "synthetic",
         "config": {"workload": "block steps of one system (C2)", "n": n,
                    "block_steps": args.bs_steps, "active_mean": float(act_n.mean()),
                    "active_min": int(act_n.min()), "active_max": int(act_n.max()),
@@ -517,6 +524,19 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+def spatial_mode() -> int:
+    """Spatial mode the library opens with (SAPPORO_B200_SPATIAL, default 1)."""
+    v = os.environ.get("SAPPORO_B200_SPATIAL")
+    return 1 if v is None else (0 if int(v) == 0 else min(int(v), 2))
+
+
+def spatial_on(ni: int, nj: int) -> bool:
+    """Whether a mixed-precision force call of ni x nj pairs runs in spatial
+    mode (the library's rule: mode 2, or mode 1 and >= 2^28 pairs)."""
+    m = spatial_mode()
+    return m == 2 or (m == 1 and ni >= 1024 and nj >= 1024 and ni * nj >= 1 << 28)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -544,7 +564,12 @@ def main():
                     help="force-kernel shape override tpi,ip,slices (default: planner)")
     ap.add_argument("--only", choices=["all", "mixed", "fp64"], default="all",
                     help="mixed / fp64: time only that device arm (profiling runs)")
+    ap.add_argument("--spatial", type=int, choices=[0, 1, 2], default=None,
+                    help="spatial mode of the mixed-precision calls (default: the library's, "
+                         "SAPPORO_B200_SPATIAL or 1)")
     args = ap.parse_args()
+    if args.spatial is not None:
+        os.environ["SAPPORO_B200_SPATIAL"] = str(args.spatial)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -663,13 +688,20 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "strong" if sharded else "weak",
         "vs_baseline": None,
-        "dtype": "f32 body + ds positions + f64 sums", "data": "synthetic",
+        "dtype": "f32 body + ds positions (near tiles) + f64 sums", "data": "synthetic",
         "config": {"workload": "precision form: Plummer N=2^20, Salpeter masses 0.1-100, 10% "
                                "circular binaries a~logU(1e-6,1e-4), Hermite 6th order, all i "
                                "active, NN on, lists off",
-                   "n": n, "order": 6, "precision": "mixed (DS dr, FP32 body, FP64 sums)",
+                   "n": n, "order": 6, "precision": "mixed (DS dr on near tiles, FP32 body, FP64 sums)",
                    "eps2": cfg["eps2"], "l2": "flushed between steps (256 MB write, then 256 MB read)",
                    "launch_plan": mix["plan"],
+                   "spatial": {"mode": spatial_mode(), "used": mix["spatial"],
+                               "far_tile_fraction": mix["far_fraction"],
+                               "delta": 1e-6,
+                               "note": "Morton-ordered j and i; (warp, j tile) pairs whose boxes "
+                                       "are >= |x|max*2^-23/delta apart take the single-float "
+                                       "position difference; the orderings (incl. two CUB "
+                                       "radix sorts) are inside the timed force call"},
                    "parallelism": (f"j-shards x{world} (round-robin j, NCCL all-reduce of "
                                    "partial forces and nearest-neighbour keys)") if sharded
                    else f"replicas x{world}",

@@ -236,6 +236,27 @@ int sapb_mlp_train(sapb_mlp *m, int n, const float *x, const float *t, int epoch
 int sapb_set_launch(sapb_dev *d, int tpi, int ip, int nslices);
 int sapb_get_plan(sapb_dev *d, int ni, int nj, int *tpi, int *ip, int *nslices);
 
+/* Spatial mode of the mixed-precision (DOUBLESINGLE) force calls: j records
+ * and i positions are taken in Morton order, and (warp, j tile) pairs whose
+ * boxes are at least |x|max * 2^-23 / delta apart use the single-float
+ * difference of the high position parts instead of the double-single one of
+ * the reference (kernels.cu:169-177), which is then accurate to delta
+ * relative.  Tiles that could hold a nearest neighbour or a list member
+ * always take the double-single path, so those results are unchanged; the
+ * force sums change only at the rounding level (the summation order too).
+ * mode 0: off (address order, the reference's arithmetic for every pair),
+ * 1: on for calls of >= 2^28 pairs (the default), 2: on for every call.
+ * delta 0 keeps the default 1e-6; at most 1e-3.  The environment variable
+ * SAPPORO_B200_SPATIAL (0, 1, 2) sets the mode at open.  Not used by
+ * sapb_force_device_noalloc or the batch calls. */
+int sapb_set_spatial(sapb_dev *d, int mode, double delta);
+/* Work of the spatial-mode calls since the last reset: (warp, j tile) pairs
+ * that took the far path and all (warp, j tile) pairs of those calls (the
+ * packed shapes; 0 and 0 before any spatial call).  Synchronises the
+ * handle's stream; reset != 0 zeroes the counters. */
+int sapb_spatial_stats(sapb_dev *d, unsigned long long *far_tiles,
+                       unsigned long long *warp_tiles, int reset);
+
 #ifdef __cplusplus
 }
 #endif

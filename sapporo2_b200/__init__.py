@@ -92,6 +92,9 @@ _SIGS = [
                                             C.c_void_p]),
     ("sapb_read_j", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _dp]),
     ("sapb_set_launch", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    ("sapb_set_spatial", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("sapb_spatial_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong),
+                                     C.POINTER(C.c_ulonglong), C.c_int]),
     ("sapb_get_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 3),
     ("sapb_batch_create", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     ("sapb_batch_destroy", C.c_int, [C.c_void_p]),
@@ -385,6 +388,22 @@ class Sapporo:
     # lower level
     def set_launch(self, tpi=0, ip=0, nslices=0):
         _check(self.lib.sapb_set_launch(self.dev, tpi, ip, nslices), "set_launch", self.dev)
+
+    def set_spatial(self, mode=1, delta=0.0):
+        """Spatial mode of the mixed-precision force calls: 0 off (address
+        order, double-single difference for every pair), 1 on for calls of
+        >= 2^28 pairs (default), 2 on for every call; far tiles use the
+        single-float difference, accurate to `delta` (0: 1e-6)."""
+        _check(self.lib.sapb_set_spatial(self.dev, int(mode), float(delta)), "set_spatial",
+               self.dev)
+
+    def spatial_stats(self, reset=False):
+        """(far, all) (warp, j tile) pairs of the spatial-mode calls since the
+        last reset."""
+        f, a = C.c_ulonglong(), C.c_ulonglong()
+        _check(self.lib.sapb_spatial_stats(self.dev, C.byref(f), C.byref(a), int(reset)),
+               "spatial_stats", self.dev)
+        return f.value, a.value
 
     def plan(self, ni, nj):
         t, i, s = C.c_int(), C.c_int(), C.c_int()

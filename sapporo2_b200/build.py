@@ -40,7 +40,7 @@ CXX_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra", f"-I{INCLUDE}", f
              f"-I{CUDA_HOME / 'include'}"]
 
 CU_SOURCES = ["sapb_kernels.cu", "sapb_capi.cu", "sapb_batch_kernels.cu", "sapb_batch.cu",
-              "sapb_mlp.cu"]
+              "sapb_mlp.cu", "sapb_spatial.cu"]
 CXX_SOURCES = ["sapporohostclass.cpp", "sapporoG6lib.cpp", "sapporoG5lib.cpp", "sapporo_cbind.cpp"]
 
 

@@ -312,6 +312,7 @@ int sapb_batch_run(sapb_batch *b, int flags) {
   const size_t used_i = b->off_i + sizeof(double) * istr * (size_t)b->total_i;
   BK(b, cudaMemcpyAsync(b->blob_d, b->blob_h, used_i, cudaMemcpyHostToDevice, d->stream));
   BK(b, cudaGraphLaunch(b->exec, d->stream));
+  if (predict) d->pred_gen++;  // the graph's predictor rewrote the records
   if (b->total_i > 0)
     BK(b, cudaMemcpyAsync(b->res_h, b->res_d, sizeof(double) * kResStride * (size_t)b->total_i,
                           cudaMemcpyDeviceToHost, d->stream));

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
   uint64_t *empty = full + kNS;
-  unsigned char *tiles = smem + 128;
+  unsigned char *tiles = smem + kHdr;
   double *tot = reinterpret_cast<double *>(tiles + C::BODY);
   __shared__ int s_item;
 

@@ -2,6 +2,7 @@
 // Declared in include/sapporo_b200.h.
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -15,6 +16,10 @@
 using namespace sapb;
 
 static char g_err[512];
+
+// Default accuracy bound of the single-float position difference on far
+// tiles (relative to the pair distance).
+constexpr double kSpatialDelta = 1e-6;
 
 static int fail(sapb_dev *d, int code, const char *fmt, ...) {
   char *buf = d ? d->err : g_err;
@@ -125,6 +130,7 @@ static int grow_j(sapb_dev *d, int new_cap) {
   d->jpool = pool;
   d->jid = id;
   d->pred = pred;
+  d->pred_gen++;
   d->cap = new_cap;
   bind_planes(d->js, pool, id, new_cap, d->order);
   return SAPB_OK;
@@ -349,6 +355,8 @@ int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
   d->order = order;
   d->prec = precision;
   d->n_pipes = n_pipes > 0 ? n_pipes : SAPB_NPIPES;
+  d->sp.far_c = (float)(0x1p-23 / kSpatialDelta);
+  if (const char *e = getenv("SAPPORO_B200_SPATIAL")) d->sp.mode = atoi(e) == 0 ? 0 : (atoi(e) >= 2 ? 2 : 1);
   int rc = SAPB_OK;
   do {
     if (cudaSetDevice(device) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "cudaSetDevice(%d)", device); break; }
@@ -393,6 +401,7 @@ int sapb_close(sapb_dev *d) {
   cudaSetDevice(d->device);
   if (d->stream) cudaStreamSynchronize(d->stream);
   free_j(d);
+  spatial_free(d);
   if (d->stage_h) cudaFreeHost(d->stage_h);
   if (d->stage_d) cudaFree(d->stage_d);
   if (d->irec_h) cudaFreeHost(d->irec_h);
@@ -484,6 +493,7 @@ int sapb_push_j(sapb_dev *d, int n) {
                         cudaMemcpyHostToDevice, d->stream));
   CK(d, launch_scatter(d->order, d->prec, d->stage_d, n, d->cap, d->js, d->pred, d->status_d,
                        d->stream));
+  d->pred_gen++;
   // the host may overwrite the staging buffer once the copy has been consumed
   CK(d, cudaStreamSynchronize(d->stream));
   return SAPB_OK;
@@ -493,6 +503,7 @@ int sapb_predict(sapb_dev *d, int nj, double ti) {
   if (!d || nj < 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "predict of %d j (capacity %d)", nj, d ? d->cap : 0);
   CK(d, cudaSetDevice(d->device));
   CK(d, launch_predict(d->order, d->prec, nj, ti, d->js, d->pred, d->stream));
+  d->pred_gen++;
   return SAPB_OK;
 }
 
@@ -506,6 +517,16 @@ double *sapb_i_stage(sapb_dev *d, int ni) {
   return d->irec_h;
 }
 
+// Spatial mode pays for its orderings (a few sorts, ~0.1 ms at 2^20) once a
+// call has this many pairs; below it the calls run in address order.
+constexpr double kSpatialMinPairs = 268435456.0;  // 2^28
+
+static bool use_spatial(const sapb_dev *d, int ni, int nj) {
+  if (d->prec != DOUBLESINGLE || d->sp.mode == 0) return false;
+  if (d->sp.mode == 2) return true;
+  return ni >= 1024 && nj >= 4 * force_tile_j() && (double)ni * nj >= kSpatialMinPairs;
+}
+
 static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
                      double *res_dev, int *cnt_dev, int *list_dev) {
   if (nj <= 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "nj = %d (capacity %d)", nj, d->cap);
@@ -514,12 +535,21 @@ static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double ep
   if (list) CK(d, cudaMemsetAsync(cnt_dev, 0, sizeof(int) * (size_t)ni, d->stream));
   ForceArgs A{};
   A.pred = d->pred;
+  if (use_spatial(d, ni, nj)) {
+    int rc = spatial_prepare(d, nj, ni, i_dev);
+    if (rc) return rc;
+    A.pred = d->sp.spred;
+    A.iperm = d->sp.iidx[1];
+    A.ibound = d->sp.ibound;
+    A.tbox = d->sp.tbox;
+    A.far_c = d->sp.far_c;
+    A.stats = d->sp.stats;
+  }
   A.nj = nj;
   A.irec = i_dev;
   A.ni = ni;
   A.eps2 = eps2;
   A.nslices = P.ns;
-  A.slice_tiles = P.slice_tiles;
   A.i_tiles = P.i_tiles;
   A.do_list = list ? 1 : 0;
   A.ngb_count = cnt_dev;
@@ -660,7 +690,6 @@ int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, 
   A.ni = ni;
   A.eps2 = eps2;
   A.nslices = P.ns;
-  A.slice_tiles = P.slice_tiles;
   A.i_tiles = P.i_tiles;
   A.do_list = list ? 1 : 0;
   A.ngb_count = ngb_count_dev;
@@ -671,6 +700,30 @@ int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, 
   CK(d, launch_force(d->order, d->prec, A, P.tpi, P.ip, d->stream));
   ReduceArgs R{scratch, P.ns, ni, res_dev, ngb_count_dev};
   CK(d, launch_reduce(R, d->stream));
+  return SAPB_OK;
+}
+
+int sapb_set_spatial(sapb_dev *d, int mode, double delta) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  if (mode < 0 || mode > 2 || !(delta >= 0.0) || delta > 1e-3)
+    return fail(d, SAPB_EINVAL, "spatial mode %d, delta %g (mode 0..2, delta 0..1e-3)", mode, delta);
+  d->sp.mode = mode;
+  d->sp.far_c = (float)(0x1p-23 / (delta > 0.0 ? delta : kSpatialDelta));
+  return SAPB_OK;
+}
+
+int sapb_spatial_stats(sapb_dev *d, unsigned long long *far_tiles,
+                       unsigned long long *warp_tiles, int reset) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  CK(d, cudaSetDevice(d->device));
+  unsigned long long h[2] = {0, 0};
+  if (d->sp.stats) {
+    CK(d, cudaMemcpyAsync(h, d->sp.stats, sizeof h, cudaMemcpyDeviceToHost, d->stream));
+    if (reset) CK(d, cudaMemsetAsync(d->sp.stats, 0, sizeof h, d->stream));
+    CK(d, cudaStreamSynchronize(d->stream));
+  }
+  if (far_tiles) *far_tiles = h[0];
+  if (warp_tiles) *warp_tiles = h[1];
   return SAPB_OK;
 }
 

@@ -64,8 +64,7 @@ struct ForceArgs {
   const double *irec; // i records
   int ni;
   double eps2;
-  int nslices;        // S: j slices across blocks
-  int slice_tiles;    // tiles per slice
+  int nslices;        // S: j slices across blocks (slice s: tiles s, s+S, ...)
   int i_tiles;        // number of i tiles
   double *out;        // results (S == 1) or partials (S > 1)
   int write_partials; // 1: write 12-double partial records per (slice, i)
@@ -73,6 +72,14 @@ struct ForceArgs {
   int *ngb_count;     // [ni] (zeroed before launch)
   int *ngb_list;      // [ni * 256]
   int *status;        // device error word
+  // Spatial mode (mixed precision; tbox == nullptr: off).  The j records of
+  // `pred` are in Morton order; i position g of the launch is i record
+  // iperm[g] (results and lists are written at iperm[g] too).
+  const int *iperm;     // [ni] (nullptr: identity)
+  const float *ibound;  // [ni] upper bound of the nearest-neighbour ds2 of i position g
+  const float4 *tbox;   // [2 * tiles]: {min xyz, max |x|}, {max xyz, 0} of the high parts
+  float far_c;          // 2^-23 / delta: far tiles are >= far_c * |x|max from every i
+  unsigned long long *stats;  // [2]: += far (warp, tile) pairs, += all (warp, tile) pairs
 };
 
 // ---- batched execution (block steps, ensembles of independent clusters) ----

@@ -101,8 +101,8 @@ __global__ void __launch_bounds__(256) readj_kernel(int first, int n, double ti,
 //
 // Block = 4 warps, laid out as TPI rows x TIT = 128/TPI columns; each thread
 // owns IP i-particles (columns tx, tx+TIT, ...), so a block covers an i-tile
-// of TI = TIT*IP particles.  blockIdx.y selects a j-slice of `slice_tiles`
-// tiles of kTJ = 256 records.  Lane 0 of warp 0 streams the slice's tiles
+// of TI = TIT*IP particles.  blockIdx.y selects j-slice s of S: the tiles
+// s, s+S, s+2S, ... of kTJ = 256 records.  Lane 0 of warp 0 streams them
 // into a 3-stage shared-memory ring with cp.async.bulk (TMA engine): `full`
 // mbarriers signal arrival (complete_tx), `empty` mbarriers collect one
 // arrival per warp; there is no block-wide barrier per tile, so warps drift
@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
   uint64_t *empty = full + kNS;
-  unsigned char *tiles = smem + 128;
+  float4 *sbox = reinterpret_cast<float4 *>(smem + 64);  // spatial mode: box of each stage's tile
+  unsigned char *tiles = smem + kHdr;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -151,10 +152,14 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 
   // ---- j range of this slice ----
   const int ntiles_all = (A.nj + kTJ - 1) / kTJ;
-  const int t0 = slice * A.slice_tiles;
-  const int t1 = min(t0 + A.slice_tiles, ntiles_all);
-  const int nt = max(t1 - t0, 0);
+  // slice s takes tiles s, s + S, s + 2S, ... (interleaved: in spatial mode
+  // the tiles near a block's i, which run slower, are spread over all slices
+  // instead of loading a few of them)
+  const int S = A.nslices;
+  const int nt = slice < ntiles_all ? (ntiles_all - slice + S - 1) / S : 0;
   const unsigned char *pred = reinterpret_cast<const unsigned char *>(A.pred);
+  // spatial mode: far tiles take the single-float difference (pair_mix2_far)
+  const bool spatial = PREC != DOUBLE && (IP % 2 == 0) && A.tbox != nullptr;
 
   if (tid == 0) {
 #pragma unroll
@@ -169,12 +174,13 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   // ---- producer: lane 0 of warp 0 fills the ring ----
   auto issue = [&](int it) {
     const int st = it % kNS;
-    const int tile = t0 + it;
+    const int tile = slice + it * S;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
     const uint32_t bytes = (uint32_t)(cnt * C::REC);
     fence_proxy_async();
-    mbar_expect_tx(&full[st], bytes);
+    mbar_expect_tx(&full[st], bytes + (spatial ? 32u : 0u));
     bulk_g2s(tiles + st * C::TILE_BYTES, pred + (size_t)tile * kTJ * C::REC, bytes, &full[st]);
+    if (spatial) bulk_g2s(sbox + 2 * st, A.tbox + 2 * tile, 32u, &full[st]);
   };
   const bool producer = (tid == 0);
   if (producer)
@@ -184,7 +190,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   const int tx = tid % C::TIT;
   const int ty = tid / C::TIT;
   const int istr = i_stride(ORDER);
-  int gi[IP];
+  int gi[IP];  // i position within the launch (Morton order in spatial mode)
+  int oi[IP];  // its i record, result and list row
   bool valid[IP];
   IMix Im[IP];
   IDp Id[IP];
@@ -194,7 +201,9 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   for (int p = 0; p < IP; p++) {
     gi[p] = itile * C::TI + p * C::TIT + tx;
     valid[p] = gi[p] < A.ni;
-    const double *r = A.irec + (size_t)(valid[p] ? gi[p] : 0) * istr;
+    // (spatial mode is mixed precision only: the FP64 kernels keep address order)
+    oi[p] = (PREC != DOUBLE && valid[p] && A.iperm) ? __ldg(A.iperm + gi[p]) : gi[p];
+    const double *r = A.irec + (size_t)(valid[p] ? oi[p] : 0) * istr;
     const double x = r[0], y = r[1], z = r[2], h2 = r[3];
     const double vx = r[4], vy = r[5], vz = r[6];
     const int id = __double2loint(r[7]);
@@ -232,7 +241,23 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 #pragma unroll
     for (int q = 0; q < NPAIR; q++) I2[q] = pack_i2(Im[2 * q], Im[(2 * q + 1) % IP]);
   }
+
+  // ---- spatial mode: what a far tile must stay clear of, per i ----
+  // A tile is far when, for every i of the warp, (1) its distance to the
+  // tile's box is at least far_c * max(|xi|, |xj|) (single-float difference
+  // accurate to delta) and (2) its squared distance, less a 1e-4 margin,
+  // exceeds lim = max(an upper bound of its nearest-neighbour ds2, h2 when
+  // lists are built): no pair of the tile can then be a nearest neighbour
+  // or a list member.  The warp votes, so the decision is warp-uniform.
+  float lim[IP];
+#pragma unroll
+  for (int p = 0; p < IP; p++) {
+    lim[p] = -1.f;
+    if (spatial && ORDER != GRAPE5 && valid[p])
+      lim[p] = fmaxf(__ldg(A.ibound + gi[p]), A.do_list ? Im[p].h2 : -1.f);
+  }
   bool broken = false;
+  int nfar = 0;  // far tiles of this warp (spatial mode)
 
   for (int it = 0; it < nt; it++) {
     const int s = it % kNS;
@@ -240,7 +265,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
       broken = true;
       atomicOr(A.status, kErrWaitTimeout);
     }
-    const int tile = t0 + it;
+    const int tile = slice + it * S;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
     const unsigned char *buf = tiles + s * C::TILE_BYTES;
 
@@ -265,7 +290,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           best_tile[p] = it;
         }
         if (A.do_list)
-          list_rescan_dp<C::RS>(Id[p], tmin[p] < Id[p].h2, gi[p], ty, TPI, rec, cnt, lane,
+          list_rescan_dp<C::RS>(Id[p], tmin[p] < Id[p].h2, oi[p], ty, TPI, rec, cnt, lane,
                                 A.ngb_count, A.ngb_list);
       }
     } else {
@@ -286,15 +311,46 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           Q[q] = AccMix2{z2, z2, z2, z2, z2, z2, z2, z2, z2, z2};
           tm[q] = make_float2(FLT_MAX, FLT_MAX);
         }
-        SAPB_UNROLL(SAPB_JUNROLL)
-        for (int k = ty; k < cnt; k += TPI) {
-          const float4 r0 = rec[k * C::RS + 0];
-          const float4 r1 = rec[k * C::RS + 1];
-          const float4 r2 = rec[k * C::RS + 2];
-          const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+        bool far = false;
+        if (spatial) {
+          const float4 bl = sbox[2 * s], bh = sbox[2 * s + 1];
+          bool ok = true;
 #pragma unroll
-          for (int q = 0; q < NPAIR; q++)
-            pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
+          for (int p = 0; p < IP; p++) {
+            const float xh = Im[p].xh, yh = Im[p].yh, zh = Im[p].zh;
+            const float gx = fmaxf(0.f, fmaxf(bl.x - xh, xh - bh.x));
+            const float gy = fmaxf(0.f, fmaxf(bl.y - yh, yh - bh.y));
+            const float gz = fmaxf(0.f, fmaxf(bl.z - zh, zh - bh.z));
+            const float g2 = fmaf(gz, gz, fmaf(gy, gy, gx * gx));
+            const float xa = fmaxf(fabsf(xh), fmaxf(fabsf(yh), fabsf(zh)));
+            const float xm = fmaxf(bl.w, xa) * A.far_c;
+            ok = ok && (!valid[p] || (g2 >= xm * xm && g2 * 0.9999f > lim[p]));
+          }
+          far = __all_sync(0xffffffffu, ok);
+          nfar += far ? 1 : 0;
+        }
+        if (far) {
+          SAPB_UNROLL(SAPB_JUNROLL)
+          for (int k = ty; k < cnt; k += TPI) {
+            const float4 r0 = rec[k * C::RS + 0];
+            const float4 r1 = rec[k * C::RS + 1];
+            const float4 r2 = rec[k * C::RS + 2];
+            const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+#pragma unroll
+            for (int q = 0; q < NPAIR; q++)
+              pair_mix2_far<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q]);
+          }
+        } else {
+          SAPB_UNROLL(SAPB_JUNROLL)
+          for (int k = ty; k < cnt; k += TPI) {
+            const float4 r0 = rec[k * C::RS + 0];
+            const float4 r1 = rec[k * C::RS + 1];
+            const float4 r2 = rec[k * C::RS + 2];
+            const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+#pragma unroll
+            for (int q = 0; q < NPAIR; q++)
+              pair_mix2<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
+          }
         }
 #pragma unroll
         for (int q = 0; q < NPAIR; q++) {
@@ -338,7 +394,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
             best_tile[p] = it;
           }
           if (A.do_list)
-            list_rescan_mix<C::RS>(Im[p], tmin[p] < Im[p].h2, gi[p], ty, TPI, rec, cnt, lane,
+            list_rescan_mix<C::RS>(Im[p], tmin[p] < Im[p].h2, oi[p], ty, TPI, rec, cnt, lane,
                                    A.ngb_count, A.ngb_list);
         }
       }
@@ -355,6 +411,10 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
         atomicOr(A.status, kErrWaitTimeout);
       }
     }
+  }
+  if (spatial && A.stats && lane == 0) {
+    atomicAdd(A.stats, (unsigned long long)nfar);
+    atomicAdd(A.stats + 1, (unsigned long long)nt);
   }
   if (broken && tid == 0) {
     // let copies still in flight land before shared memory is released
@@ -377,7 +437,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   for (int p = 0; p < IP; p++) {
     key[p] = nn_key(kNoNgbDs2, -1);
     if (best_tile[p] < 0) continue;
-    const int tile = t0 + best_tile[p];
+    const int tile = slice + best_tile[p] * S;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
     if (PREC == DOUBLE) {
       const double4 *rec = reinterpret_cast<const double4 *>(pred + (size_t)tile * kTJ * C::REC);
@@ -430,8 +490,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 #pragma unroll
   for (int p = 0; p < IP; p++) {
     if (!valid[p]) continue;
-    double *o = A.write_partials ? A.out + ((size_t)slice * A.ni + gi[p]) * kResStride
-                                 : A.out + (size_t)gi[p] * kResStride;
+    double *o = A.write_partials ? A.out + ((size_t)slice * A.ni + oi[p]) * kResStride
+                                 : A.out + (size_t)oi[p] * kResStride;
     o[0] = D[p].ax; o[1] = D[p].ay; o[2] = D[p].az; o[3] = D[p].pot;
     o[4] = D[p].jx; o[5] = D[p].jy; o[6] = D[p].jz;
     o[7] = D[p].sx; o[8] = D[p].sy; o[9] = D[p].sz;
@@ -564,11 +624,13 @@ static cudaError_t launch_force_t(const ForceArgs *A, cudaStream_t st, int *occ)
 // one instantiation.
 template <int ORDER, int PREC>
 static cudaError_t launch_force_o(const ForceArgs *A, int tpi, int ip, cudaStream_t st, int *occ) {
-  if (ip == 4 && PREC != DOUBLE) {
-    switch (tpi) {
-      case 1: return launch_force_t<ORDER, PREC, 1, 4>(A, st, occ);
-      case 2: return launch_force_t<ORDER, PREC, 2, 4>(A, st, occ);
-      default: break;
+  if (ip == 4) {
+    if constexpr (PREC != DOUBLE) {  // 4 i per thread: mixed precision only
+      switch (tpi) {
+        case 1: return launch_force_t<ORDER, PREC, 1, 4>(A, st, occ);
+        case 2: return launch_force_t<ORDER, PREC, 2, 4>(A, st, occ);
+        default: break;
+      }
     }
   } else if (ip == 2) {
     switch (tpi) {

@@ -61,6 +61,10 @@ __device__ __forceinline__ void taylor(const JState &js, int k, double ti, doubl
 constexpr int kBT = 128;
 constexpr int kTJ = 256;
 constexpr int kNS = 3;
+// Shared-memory header of the force kernel: full/empty mbarriers of the ring
+// (bytes 0..47) and, in spatial mode, the box of the tile in each stage
+// (2 float4 per stage, bytes 64..159); the tile ring starts at kHdr.
+constexpr int kHdr = 256;
 
 template <int ORDER, int PREC, int TPI, int IP>
 struct FCfg {
@@ -76,8 +80,11 @@ struct FCfg {
   // i, [field][thread] so a warp's accesses are consecutive), which frees
   // 40 registers per thread and lets 4 blocks share an SM
   static constexpr int TOT_BYTES = PREC == DOUBLE ? 0 : IP * 10 * kBT * 8;
-  static constexpr int SMEM = 128 + BODY + TOT_BYTES;
-  static constexpr int MIN_BLOCKS = PREC == DOUBLE ? 1 : (IP >= 4 ? 2 : 4);
+  static constexpr int SMEM = kHdr + BODY + TOT_BYTES;
+  // resident blocks per SM the register budget is held to: FP64 kernels sit
+  // at 168 registers, where one more allocation step (176) drops them from
+  // 3 to 2 blocks per SM and costs 7 % at N = 2^20 (6th order)
+  static constexpr int MIN_BLOCKS = PREC == DOUBLE ? 3 : (IP >= 4 ? 2 : 4);
 };
 
 // ---------------- mixed precision pair ----------------
@@ -271,6 +278,32 @@ __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, cons
                                           const float4 &r2, const float4 &r3, float2 eps2,
                                           AccMix2 &A, float2 &tmin) {
   const Pre2 P = pair_mix2_pre<ORDER != GRAPE5>(I, r0, r1, eps2, tmin);
+  pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
+}
+
+// Far tile (spatial mode): the j tile and the warp's i are at least
+// |x|max * 2^-23 / delta apart, so the difference of the high parts alone,
+// xj_hi - xi_hi, is within delta (relative) of the double-single one (each
+// low part is below 2^-24 |x|): 3 FMA-pipe operations instead of 9.  No pair
+// of such a tile can be a nearest neighbour or a list member (the caller
+// checks that against the warp's bounds), so no ds2 minimum is kept; the
+// self pair is still masked by id.
+template <int ORDER>
+__device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, const float4 &r1,
+                                              const float4 &r2, const float4 &r3, float2 eps2,
+                                              AccMix2 &A) {
+  Pre2 P;
+  P.dx = __fadd2_rn(bc2(r0.x), I.nxh);
+  P.dy = __fadd2_rn(bc2(r0.y), I.nyh);
+  P.dz = __fadd2_rn(bc2(r0.z), I.nzh);
+  if (ORDER != GRAPE5) {
+    const int idj = __float_as_int(r1.w);
+    P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
+    P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
+  }
+  const float2 ds2 = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dx, P.dx)));
+  const float2 r2v = __fadd2_rn(ds2, eps2);
+  P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
   pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
 

@@ -53,15 +53,18 @@ def oracle_force(case: dict, sel=None, lists=True) -> dict:
                    case["id"], case["eps2"], lists=lists)
 
 
-def run_library(case: dict, precision: int, sel=None, lists=True, launch=None) -> dict:
+def run_library(case: dict, precision: int, sel=None, lists=True, launch=None,
+                spatial=None) -> dict:
     """Drives the sapporo class exactly as an integrator would: stage all j,
     set_time, startGravCalc on the selected i, getGravResults, neighbour
-    readout."""
+    readout.  `spatial` = (mode, delta) sets the spatial mode first."""
     import sapporo2_b200 as sp
     o, n = case["order"], case["n"]
     with sp.Sapporo(order=o, precision=precision) as s:
         if launch:
             s.set_launch(*launch)
+        if spatial is not None:
+            s.set_spatial(*spatial)
         s.set_j_particles(np.arange(n), case["id"], case["t0"], case["m"], case["x"], case["v"],
                           case["a"], case["j"], case["s"], case["c"])
         s.set_time(case["ti"])
@@ -70,6 +73,7 @@ def run_library(case: dict, precision: int, sel=None, lists=True, launch=None) -
                 case["pa"][idx] if case["pa"] is not None else None, case["eps2"],
                 case["h2"][idx])
         r = s.results(n, ngb=True)
+        r["raw"] = s.raw_results(len(idx)).copy()
         if lists:
             r["overflow"] = s.read_ngb_list()
             cnts, lsts = [], []

@@ -1,0 +1,134 @@
+"""GPU: spatial mode of the mixed-precision force calls.
+
+In spatial mode the predicted j records and the call's i positions are taken
+in Morton order, and (warp, j tile) pairs whose boxes are far apart use the
+single-float difference of the high position parts instead of the
+double-single difference of the reference (kernels.cu:169-177).  Tiles that
+could hold a nearest neighbour or a list member always take the
+double-single path.  So, against the same call in address order (mode 0):
+nearest neighbours, their ds2 and the neighbour lists are identical, and the
+forces agree with the FP64 oracle within the mixed-precision tolerance.
+"""
+import numpy as np
+import pytest
+
+import sapporo2_b200 as sp
+from tests import cases as T
+
+pytestmark = pytest.mark.gpu
+
+EVERY_CALL = 2  # spatial mode for every call, whatever its size
+
+
+def _same_neighbours(a, b):
+    """Nearest neighbours (id and ds2 bits) and neighbour lists identical."""
+    assert np.array_equal(a["raw"][:, 10:12], b["raw"][:, 10:12])
+    assert np.array_equal(a["nnb"], b["nnb"])
+    assert a["overflow"] == b["overflow"]
+    assert np.array_equal(a["ngb_count"], b["ngb_count"])
+    for q in np.nonzero(np.asarray(a["ngb_count"]) < sp.NGB_PB)[0]:
+        assert np.array_equal(a["ngb_sets"][q], b["ngb_sets"][q]), q
+
+
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("delta", [0.0, 1e-5])
+def test_spatial_matches_oracle_and_address_order(gpu, order, delta):
+    case = T.build_case(order, 6000, seed=21, binaries=0.1)
+    want = T.oracle_force(case)
+    got = T.run_library(case, sp.DOUBLESINGLE, spatial=(EVERY_CALL, delta))
+    ref = T.run_library(case, sp.DOUBLESINGLE, spatial=(0, 0.0))
+    st = T.check_forces(got, want, order)
+    assert T.check_nn(case, got["nnb"], want) == T.check_nn(case, ref["nnb"], want)
+    T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want)
+    _same_neighbours(got, ref)
+    # the far path ran: the forces are not those of the address-order call
+    assert not np.array_equal(got["raw"][:, :10], ref["raw"][:, :10])
+    print(st)
+
+
+@pytest.mark.parametrize("launch", [(1, 4, 0), (2, 4, 3), (1, 2, 0), (2, 2, 3), (4, 2, 0),
+                                    (8, 2, 5), (16, 1, 2), (32, 1, 0)])
+def test_spatial_launch_shapes(gpu, launch):
+    """Every shape: the packed ones (two i per instruction) take far tiles,
+    the one-i-per-thread ones only the Morton order of i and j."""
+    case = T.build_case(2, 3000, seed=22, binaries=0.1)
+    sel = np.random.default_rng(5).choice(3000, 2500, replace=False)
+    want = T.oracle_force(case, sel=sel)
+    got = T.run_library(case, sp.DOUBLESINGLE, sel=sel, launch=launch,
+                        spatial=(EVERY_CALL, 1e-5))
+    ref = T.run_library(case, sp.DOUBLESINGLE, sel=sel, launch=launch, spatial=(0, 0.0))
+    T.check_forces(got, want, 2)
+    T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want, sel=sel)
+    _same_neighbours(got, ref)
+
+
+def test_spatial_foreign_i_outside_the_j_box(gpu):
+    """i that are not among the j (other ids) and partly far outside the j
+    box, where their Morton keys clamp to its faces."""
+    case = T.build_case(2, 4000, seed=23, binaries=0.1)
+    rng = np.random.default_rng(8)
+    ni = 3000
+    xi = case["px"][rng.choice(4000, ni)] + rng.normal(scale=1e-3, size=(ni, 3))
+    xi[: ni // 3] += np.array([40.0, -25.0, 10.0])
+    vi = rng.normal(scale=0.3, size=(ni, 3))
+    ai = rng.normal(scale=0.1, size=(ni, 3))
+    ids = np.arange(ni, dtype=np.int32) + 10_000_000
+    h2 = np.full(ni, 0.01)
+    from oracle import oracle as O
+    want = O.force(2, xi, vi, ai, h2, ids, case["px"], case["pv"], case["pa"], case["m"],
+                   case["id"], case["eps2"], lists=True)
+    out = {}
+    for mode in (EVERY_CALL, 0):
+        with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
+            s.set_spatial(mode, 1e-5)
+            n = case["n"]
+            s.set_j_particles(np.arange(n), case["id"], case["t0"], case["m"], case["x"],
+                              case["v"], case["a"], case["j"], case["s"], case["c"])
+            s.set_time(case["ti"])
+            s.start(n, ids, xi, vi, ai, case["eps2"], h2)
+            r = s.results(n, ngb=True)
+            r["raw"] = s.raw_results(ni).copy()
+            out[mode] = r
+    got = out[EVERY_CALL]
+    T.check_forces(got, want, 2)
+    assert np.array_equal(got["raw"][:, 10:12], out[0]["raw"][:, 10:12])
+    jpos = {int(k): p for k, p in zip(case["id"], case["px"])}
+    for q in np.nonzero(got["nnb"] != want["nnb"])[0]:  # near-ties only
+        d = [float(((jpos[int(k)] - xi[q]) ** 2).sum()) for k in (got["nnb"][q], want["nnb"][q])]
+        assert abs(d[0] - d[1]) <= 1e-6 * d[1], (q, d)
+
+
+def test_spatial_reorders_after_j_change(gpu):
+    """The ordering follows the predicted records: a second call after new j
+    data and a new prediction time uses them, not the first call's order."""
+    a = T.build_case(2, 5000, seed=24, binaries=0.1)
+    b = T.build_case(2, 5000, seed=25, binaries=0.1)
+    n = a["n"]
+    with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
+        s.set_spatial(EVERY_CALL, 1e-5)
+        for case in (a, b):
+            s.set_j_particles(np.arange(n), case["id"], case["t0"], case["m"], case["x"],
+                              case["v"], case["a"], case["j"], case["s"], case["c"])
+            s.set_time(case["ti"])
+            s.start(n, case["id"], case["px"], case["pv"], case["pa"], case["eps2"], case["h2"])
+            got = s.results(n, ngb=True)
+            want = T.oracle_force(case, lists=False)
+            T.check_forces(got, want, 2)
+            T.check_nn(case, got["nnb"], want)
+
+
+def test_spatial_default_mode_threshold(gpu):
+    """Mode 1 (the default) orders only calls of >= 2^28 pairs: a small call
+    gives bit-identical results to mode 0."""
+    case = T.build_case(2, 2000, seed=26, binaries=0.1)
+    got = T.run_library(case, sp.DOUBLESINGLE, spatial=(1, 0.0))
+    ref = T.run_library(case, sp.DOUBLESINGLE, spatial=(0, 0.0))
+    assert np.array_equal(got["raw"], ref["raw"])
+
+
+def test_spatial_rejects_bad_arguments(gpu):
+    with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
+        for mode, delta in [(3, 0.0), (-1, 0.0), (1, -1e-6), (1, 1e-2), (1, float("nan"))]:
+            with pytest.raises(sp.SapporoError):
+                s.set_spatial(mode, delta)
+        s.set_spatial(0, 0.0)

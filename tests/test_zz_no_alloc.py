@@ -72,6 +72,7 @@ def test_noalloc_matches_device_call_twice(gpu):
         s.set_time(case["ti"])
         s.force_prediction(n)
         lib, dev = s.lib, s.dev
+        s.set_spatial(0)  # both calls in address order: the same arithmetic per pair
         # first call: every particle
         rec1 = _records(case, np.arange(n))
         _compare(_call(lib, dev, "sapb_force_device_noalloc", n, rec1, torch),
