@@ -40,8 +40,9 @@ METRIC = "interactions/s at N=2^20 mixed vs plain FP64, 1 GPU, acc err<=1e-6; %F
 
 # DRAM bytes of one mixed 6th-order force launch at N = 2^20, all i, from
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (one pass) of
-# `bench.py --steps 1 --warmup 0 --only mixed --no-cpu`
-FORCE_DRAM_BYTES = 968.47e6 + 182.86e6
+# `bench.py --steps 1 --warmup 0 --only mixed --no-cpu` (spatial mode, and with --spatial 0)
+FORCE_DRAM_BYTES = 1060.0e6 + 176.01e6
+FORCE_DRAM_BYTES_ADDRESS_ORDER = 968.47e6 + 182.86e6
 
 
 def log(*a):
@@ -712,10 +713,13 @@ def main():
                  "speedup_mixed_over_fp64": value / jobs / f64_value},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak,
-                     "traffic": FORCE_DRAM_BYTES if (n == 1 << 20 and nj_loc == n) else None,
+                     "traffic": ((FORCE_DRAM_BYTES if mix["spatial"] else
+                                  FORCE_DRAM_BYTES_ADDRESS_ORDER)
+                                 if (n == 1 << 20 and nj_loc == n) else None),
                      "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one "
                                      "force_kernel<6th,DS> launch at N=2^20 (ncu, 1 pass): "
-                                     "968.5 MB read + 182.9 MB written in 2.03 s, 0.57 GB/s; "
+                                     "1060 MB read + 176 MB written in 1.86 s, 0.66 GB/s (spatial mode; "
+                                     "address order 968 + 183 MB in 2.03 s); "
                                      "j records stream from L2",
                      "peak_note": f"derived: {nsm} SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz "
                                   "(sm_max_mhz of measured peaks; no FP32 entry there)",
