@@ -361,8 +361,9 @@ def run_learned_h2_bench(args):
     """The learned-h2 workload: N=262144 Plummer + 10 % binaries, 6th-order
     block steps, neighbour lists on (target 32, cap 256), the same steps run
     with the fixed global radius, the count-scaled radius and the learned
-    radius.  Forces do not depend on the radius, so the three trajectories
-    are identical; the policies differ in overflows, retries and time."""
+    radius.  Forces do not depend on the radius (in spatial mode too: its
+    far test ignores h2), so the three trajectories are identical; the
+    policies differ in overflows, retries and time."""
     from sapporo2_b200 import hermite6 as H, ic
     cfg = ic.make_config("C5", n=args.c5_n, seed=5)
     policies = {"fixed": lambda: H.FixedH2(), "count_scaled": lambda: H.CountScaledH2(),

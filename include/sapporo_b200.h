@@ -241,12 +241,13 @@ int sapb_get_plan(sapb_dev *d, int ni, int nj, int *tpi, int *ip, int *nslices);
  * boxes are at least |x|max * 2^-23 / delta apart use the single-float
  * difference of the high position parts instead of the double-single one of
  * the reference (kernels.cu:169-177), which is then accurate to delta
- * relative.  Tiles that could hold a nearest neighbour or a list member
- * always take the double-single path, so those results are unchanged; the
- * force sums change only at the rounding level (the summation order too).
+ * relative.  Tiles that could hold a nearest neighbour always take the
+ * double-single path and list members on far tiles are found by an exact
+ * rescan, so neighbours and lists are unchanged; the force sums change only
+ * at the rounding level (the summation order too) and do not depend on h2.
  * mode 0: off (address order, the reference's arithmetic for every pair),
  * 1: on for calls of >= 2^28 pairs (the default), 2: on for every call.
- * delta 0 keeps the default 1e-6; at most 1e-3.  The environment variable
+ * delta 0 keeps the default 1e-6; at most 1e-4.  The environment variable
  * SAPPORO_B200_SPATIAL (0, 1, 2) sets the mode at open.  Not used by
  * sapb_force_device_noalloc or the batch calls. */
 int sapb_set_spatial(sapb_dev *d, int mode, double delta);

@@ -705,8 +705,8 @@ int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, 
 
 int sapb_set_spatial(sapb_dev *d, int mode, double delta) {
   if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
-  if (mode < 0 || mode > 2 || !(delta >= 0.0) || delta > 1e-3)
-    return fail(d, SAPB_EINVAL, "spatial mode %d, delta %g (mode 0..2, delta 0..1e-3)", mode, delta);
+  if (mode < 0 || mode > 2 || !(delta >= 0.0) || delta > 1e-4)
+    return fail(d, SAPB_EINVAL, "spatial mode %d, delta %g (mode 0..2, delta 0..1e-4)", mode, delta);
   d->sp.mode = mode;
   d->sp.far_c = (float)(0x1p-23 / (delta > 0.0 ? delta : kSpatialDelta));
   return SAPB_OK;

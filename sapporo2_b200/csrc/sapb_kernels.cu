@@ -246,16 +246,21 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   // A tile is far when, for every i of the warp, (1) its distance to the
   // tile's box is at least far_c * max(|xi|, |xj|) (single-float difference
   // accurate to delta) and (2) its squared distance, less a 1e-4 margin,
-  // exceeds lim = max(an upper bound of its nearest-neighbour ds2, h2 when
-  // lists are built): no pair of the tile can then be a nearest neighbour
-  // or a list member.  The warp votes, so the decision is warp-uniform.
+  // exceeds lim = an upper bound of its nearest-neighbour ds2: no pair of the
+  // tile can then be a nearest neighbour.  The warp votes, so the decision
+  // is warp-uniform.  It does not depend on h2, so neither do the forces:
+  // list members in far tiles are found by an exact rescan, triggered by the
+  // tile's approximate ds2 minimum.
   float lim[IP];
 #pragma unroll
   for (int p = 0; p < IP; p++) {
     lim[p] = -1.f;
-    if (spatial && ORDER != GRAPE5 && valid[p])
-      lim[p] = fmaxf(__ldg(A.ibound + gi[p]), A.do_list ? Im[p].h2 : -1.f);
+    if (spatial && ORDER != GRAPE5 && valid[p]) lim[p] = __ldg(A.ibound + gi[p]);
   }
+  // Margin of the far tests: a box distance from high parts, and a ds2 from
+  // the single-float difference, are within 2 sqrt(3) delta (relative) of the
+  // exact ones on a far tile.
+  const float shrink = spatial ? fminf(0.9999f, 1.f - 8.f * (0x1p-23f / A.far_c)) : 1.f;
   bool broken = false;
   int nfar = 0;  // far tiles of this warp (spatial mode)
 
@@ -302,6 +307,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
         P[p] = AccMix{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         tmin[p] = FLT_MAX;
       }
+      bool far = false;  // spatial mode: this tile took the single-float difference
       if constexpr (IP % 2 == 0) {
         AccMix2 Q[NPAIR];
         float2 tm[NPAIR];
@@ -311,7 +317,6 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           Q[q] = AccMix2{z2, z2, z2, z2, z2, z2, z2, z2, z2, z2};
           tm[q] = make_float2(FLT_MAX, FLT_MAX);
         }
-        bool far = false;
         if (spatial) {
           const float4 bl = sbox[2 * s], bh = sbox[2 * s + 1];
           bool ok = true;
@@ -324,12 +329,12 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
             const float g2 = fmaf(gz, gz, fmaf(gy, gy, gx * gx));
             const float xa = fmaxf(fabsf(xh), fmaxf(fabsf(yh), fabsf(zh)));
             const float xm = fmaxf(bl.w, xa) * A.far_c;
-            ok = ok && (!valid[p] || (g2 >= xm * xm && g2 * 0.9999f > lim[p]));
+            ok = ok && (!valid[p] || (g2 >= xm * xm && g2 * shrink > lim[p]));
           }
           far = __all_sync(0xffffffffu, ok);
           nfar += far ? 1 : 0;
         }
-        if (far) {
+        if (far && A.do_list && ORDER != GRAPE5) {
           SAPB_UNROLL(SAPB_JUNROLL)
           for (int k = ty; k < cnt; k += TPI) {
             const float4 r0 = rec[k * C::RS + 0];
@@ -338,7 +343,18 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
             const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
 #pragma unroll
             for (int q = 0; q < NPAIR; q++)
-              pair_mix2_far<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q]);
+              pair_mix2_far<ORDER, true>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
+          }
+        } else if (far) {
+          SAPB_UNROLL(SAPB_JUNROLL)
+          for (int k = ty; k < cnt; k += TPI) {
+            const float4 r0 = rec[k * C::RS + 0];
+            const float4 r1 = rec[k * C::RS + 1];
+            const float4 r2 = rec[k * C::RS + 2];
+            const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
+#pragma unroll
+            for (int q = 0; q < NPAIR; q++)
+              pair_mix2_far<ORDER, false>(I2[q], r0, r1, r2, r3, eps2v, Q[q], tm[q]);
           }
         } else {
           SAPB_UNROLL(SAPB_JUNROLL)
@@ -389,13 +405,16 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           t[9 * kBT] += (double)P[p].sz;
         }
         if (ORDER != GRAPE5) {  // GRAPE-5: no nearest neighbour, no lists
-          if (tmin[p] < best[p]) {
+          // a far tile holds no nearest neighbour; its minimum is the
+          // single-float ds2 (hence the margin on the rescan trigger; the
+          // rescan itself is exact)
+          if (!far && tmin[p] < best[p]) {
             best[p] = tmin[p];
             best_tile[p] = it;
           }
           if (A.do_list)
-            list_rescan_mix<C::RS>(Im[p], tmin[p] < Im[p].h2, oi[p], ty, TPI, rec, cnt, lane,
-                                   A.ngb_count, A.ngb_list);
+            list_rescan_mix<C::RS>(Im[p], (far ? tmin[p] * shrink : tmin[p]) < Im[p].h2, oi[p],
+                                   ty, TPI, rec, cnt, lane, A.ngb_count, A.ngb_list);
         }
       }
     }

@@ -117,6 +117,22 @@ def test_spatial_reorders_after_j_change(gpu):
             T.check_nn(case, got["nnb"], want)
 
 
+def test_spatial_forces_do_not_depend_on_h2(gpu):
+    """The far test ignores h2 (list members on far tiles are found by an exact
+    rescan), so two radii give bit-identical forces and nearest neighbours;
+    a radius reaching well into far tiles still gives the address-order
+    lists."""
+    case = T.build_case(2, 6000, seed=27, binaries=0.1)
+    wide = dict(case)
+    wide["h2"] = np.full(case["n"], 0.15 ** 2)
+    a = T.run_library(case, sp.DOUBLESINGLE, spatial=(EVERY_CALL, 1e-5))
+    b = T.run_library(wide, sp.DOUBLESINGLE, spatial=(EVERY_CALL, 1e-5))
+    ref = T.run_library(wide, sp.DOUBLESINGLE, spatial=(0, 0.0))
+    assert np.array_equal(a["raw"], b["raw"])
+    _same_neighbours(b, ref)
+    assert np.mean(b["ngb_count"]) > 10  # lists reach far beyond the near tiles
+
+
 def test_spatial_default_mode_threshold(gpu):
     """Mode 1 (the default) orders only calls of >= 2^28 pairs: a small call
     gives bit-identical results to mode 0."""
@@ -128,7 +144,7 @@ def test_spatial_default_mode_threshold(gpu):
 
 def test_spatial_rejects_bad_arguments(gpu):
     with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
-        for mode, delta in [(3, 0.0), (-1, 0.0), (1, -1e-6), (1, 1e-2), (1, float("nan"))]:
+        for mode, delta in [(3, 0.0), (-1, 0.0), (1, -1e-6), (1, 2e-4), (1, float("nan"))]:
             with pytest.raises(sp.SapporoError):
                 s.set_spatial(mode, delta)
         s.set_spatial(0, 0.0)
