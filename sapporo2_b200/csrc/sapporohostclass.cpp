@@ -15,9 +15,12 @@
 // more than NGB_PB entries and flags overflow when the count reaches NGB_PB.
 #include "../../include/sapporohostclass.h"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "../../include/sapporo_b200.h"
@@ -187,6 +190,33 @@ int sapporo::set_j_particle(int address, int id, double tj, double dtj, double m
   return 0;
 }
 
+// fn(begin, end) over [0, n): chunks of at least 32768 on up to 16 threads
+// (a bulk j upload of 2^20 records packs 185 MB); a thread that cannot be
+// started runs its chunk inline.
+template <class F>
+static void parallel_chunks(int n, F fn) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::max(1, std::min((int)std::min(hw, 16u), n / 32768));
+  if (nt <= 1) {
+    fn(0, n);
+    return;
+  }
+  const int step = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (int t = 1; t < nt; t++) {
+    const int b = t * step, e = std::min(n, b + step);
+    if (b >= e) continue;
+    try {
+      th.emplace_back(fn, b, e);
+    } catch (const std::system_error &) {
+      fn(b, e);
+    }
+  }
+  fn(0, std::min(n, step));
+  for (auto &x : th) x.join();
+}
+
 int sapporo::set_j_particles(int n, const int *address, const int *id, const double *t,
                              const double *mass, const double *x, const double *v,
                              const double *a, const double *jrk, const double *snp,
@@ -233,24 +263,27 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
   }
   const int ss = sapb_j_stage_stride(dev_);
   const bool six = integrationOrder > FOURTH;
-  for (int k = 0; k < n; k++) {
-    double *r = base + (size_t)slots[k] * ss;
-    put_int_pair(&r[0], address[k], id[k]);
-    r[1] = t ? t[k] : 0.0;
-    r[2] = mass[k];
-    for (int d = 0; d < 3; d++) {
-      r[3 + d] = x[3 * k + d];
-      r[6 + d] = v ? v[3 * k + d] : 0.0;
-      r[9 + d] = a ? a[3 * k + d] : 0.0;
-      r[12 + d] = jrk ? jrk[3 * k + d] : 0.0;
-    }
-    r[15] = eps ? eps[k] : 0.0;
-    if (six)
+  const int *sl = slots.data();
+  parallel_chunks(n, [=](int k0, int k1) {
+    for (int k = k0; k < k1; k++) {
+      double *r = base + (size_t)sl[k] * ss;
+      put_int_pair(&r[0], address[k], id[k]);
+      r[1] = t ? t[k] : 0.0;
+      r[2] = mass[k];
       for (int d = 0; d < 3; d++) {
-        r[16 + d] = snp ? snp[3 * k + d] : 0.0;
-        r[19 + d] = crk ? crk[3 * k + d] : 0.0;
+        r[3 + d] = x[3 * k + d];
+        r[6 + d] = v ? v[3 * k + d] : 0.0;
+        r[9 + d] = a ? a[3 * k + d] : 0.0;
+        r[12 + d] = jrk ? jrk[3 * k + d] : 0.0;
       }
-  }
+      r[15] = eps ? eps[k] : 0.0;
+      if (six)
+        for (int d = 0; d < 3; d++) {
+          r[16 + d] = snp ? snp[3 * k + d] : 0.0;
+          r[19 + d] = crk ? crk[3 * k + d] : 0.0;
+        }
+    }
+  });
   return 0;
 }
 
