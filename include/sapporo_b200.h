@@ -248,7 +248,8 @@ int sapb_get_plan(sapb_dev *d, int ni, int nj, int *tpi, int *ip, int *nslices);
  * mode 0: off (address order, the reference's arithmetic for every pair),
  * 1: on for calls of >= 2^28 pairs (the default), 2: on for every call.
  * delta 0 keeps the default 1e-6; at most 1e-4.  The environment variable
- * SAPPORO_B200_SPATIAL (0, 1, 2) sets the mode at open.  Not used by
+ * SAPPORO_B200_SPATIAL (0, 1, 2) sets the mode at open.  A call for whose
+ * sort buffers the device has no room runs in address order.  Not used by
  * sapb_force_device_noalloc or the batch calls. */
 int sapb_set_spatial(sapb_dev *d, int mode, double delta);
 /* Work of the spatial-mode calls since the last reset: (warp, j tile) pairs

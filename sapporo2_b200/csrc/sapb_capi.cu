@@ -535,9 +535,13 @@ static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double ep
   if (list) CK(d, cudaMemsetAsync(cnt_dev, 0, sizeof(int) * (size_t)ni, d->stream));
   ForceArgs A{};
   A.pred = d->pred;
-  if (use_spatial(d, ni, nj)) {
-    int rc = spatial_prepare(d, nj, ni, i_dev);
-    if (rc) return rc;
+  bool spatial = use_spatial(d, ni, nj);
+  if (spatial) {
+    const int rc = spatial_prepare(d, nj, ni, i_dev);
+    if (rc == SAPB_ENOMEM) spatial = false;  // no room for its buffers: address order
+    else if (rc) return rc;
+  }
+  if (spatial) {
     A.pred = d->sp.spred;
     A.iperm = d->sp.iidx[1];
     A.ibound = d->sp.ibound;
