@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   using C = FCfg<ORDER, PREC, TPI, IP>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  uint64_t *empty = full + kNS;
+  uint64_t *empty = full + C::NS;
   float4 *sbox = reinterpret_cast<float4 *>(smem + 64);  // spatial mode: box of each stage's tile
   unsigned char *tiles = smem + kHdr;
 
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < kNS; s++) {
+    for (int s = 0; s < C::NS; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kBT / 32);
     }
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 
   // ---- producer: lane 0 of warp 0 fills the ring ----
   auto issue = [&](int it) {
-    const int st = it % kNS;
+    const int st = it % C::NS;
     const int tile = slice + it * S;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
     const uint32_t bytes = (uint32_t)(cnt * C::REC);
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   };
   const bool producer = (tid == 0);
   if (producer)
-    for (int it = 0; it < kNS && it < nt; it++) issue(it);
+    for (int it = 0; it < C::NS && it < nt; it++) issue(it);
 
   // ---- consumers: 128 threads = TPI rows x TIT columns, IP i each ----
   const int tx = tid % C::TIT;
@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   int nfar = 0;  // far tiles of this warp (spatial mode)
 
   for (int it = 0; it < nt; it++) {
-    const int s = it % kNS;
-    if (!broken && !mbar_wait_bounded(&full[s], (uint32_t)((it / kNS) & 1))) {
+    const int s = it % C::NS;
+    if (!broken && !mbar_wait_bounded(&full[s], (uint32_t)((it / C::NS) & 1))) {
       broken = true;
       atomicOr(A.status, kErrWaitTimeout);
     }
@@ -421,10 +421,10 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
     // Refill the stage once all four warps released it; only warp 0 waits
-    // here, the others may already be up to kNS-1 tiles ahead.
-    if (producer && !broken && it + kNS < nt) {
-      if (mbar_wait_bounded(&empty[s], (uint32_t)((it / kNS) & 1))) {
-        issue(it + kNS);
+    // here, the others may already be up to C::NS-1 tiles ahead.
+    if (producer && !broken && it + C::NS < nt) {
+      if (mbar_wait_bounded(&empty[s], (uint32_t)((it / C::NS) & 1))) {
+        issue(it + C::NS);
       } else {
         broken = true;
         atomicOr(A.status, kErrWaitTimeout);
@@ -437,8 +437,8 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   }
   if (broken && tid == 0) {
     // let copies still in flight land before shared memory is released
-    for (int it = max(nt - kNS, 0); it < nt; it++)
-      mbar_wait_bounded(&full[it % kNS], (uint32_t)((it / kNS) & 1));
+    for (int it = max(nt - C::NS, 0); it < nt; it++)
+      mbar_wait_bounded(&full[it % C::NS], (uint32_t)((it / C::NS) & 1));
   }
 
   if (PREC != DOUBLE) {  // mixed sums of acc, jerk, snap carry -1/tau (kTau)

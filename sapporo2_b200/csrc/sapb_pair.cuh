@@ -85,7 +85,8 @@ struct FCfg {
   static constexpr int REC = RS * FB;
   static constexpr int TILE_BYTES = kTJ * REC;
   static constexpr int RED_BYTES = TPI > 1 ? kBT * IP * kResStride * 8 : 0;
-  static constexpr int BODY = kNS * TILE_BYTES > RED_BYTES ? kNS * TILE_BYTES : RED_BYTES;
+  static constexpr int NS = kNS;  // stages of the tile ring
+  static constexpr int BODY = NS * TILE_BYTES > RED_BYTES ? NS * TILE_BYTES : RED_BYTES;
   // mixed precision keeps its FP64 running totals in shared memory (10 per
   // i, [field][thread] so a warp's accesses are consecutive), which frees
   // 40 registers per thread and lets 4 blocks share an SM
