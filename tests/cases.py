@@ -74,6 +74,8 @@ def run_library(case: dict, precision: int, sel=None, lists=True, launch=None,
                 case["h2"][idx])
         r = s.results(n, ngb=True)
         r["raw"] = s.raw_results(len(idx)).copy()
+        if spatial is not None:
+            r["far_tiles"] = s.spatial_stats()  # (far, all) (warp, tile) pairs
         if lists:
             r["overflow"] = s.read_ngb_list()
             cnts, lsts = [], []

@@ -33,17 +33,19 @@ def _same_neighbours(a, b):
 @pytest.mark.parametrize("order", [1, 2])
 @pytest.mark.parametrize("delta", [0.0, 1e-5])
 def test_spatial_matches_oracle_and_address_order(gpu, order, delta):
+    """Shape (1, 4): at this size the planner would pick one i per thread,
+    which takes the Morton order but not the far tiles."""
     case = T.build_case(order, 6000, seed=21, binaries=0.1)
     want = T.oracle_force(case)
-    got = T.run_library(case, sp.DOUBLESINGLE, spatial=(EVERY_CALL, delta))
-    ref = T.run_library(case, sp.DOUBLESINGLE, spatial=(0, 0.0))
+    got = T.run_library(case, sp.DOUBLESINGLE, launch=(1, 4, 0), spatial=(EVERY_CALL, delta))
+    ref = T.run_library(case, sp.DOUBLESINGLE, launch=(1, 4, 0), spatial=(0, 0.0))
     st = T.check_forces(got, want, order)
     assert T.check_nn(case, got["nnb"], want) == T.check_nn(case, ref["nnb"], want)
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want)
     _same_neighbours(got, ref)
-    # the far path ran: the forces are not those of the address-order call
-    assert not np.array_equal(got["raw"][:, :10], ref["raw"][:, :10])
-    print(st)
+    far, tiles = got["far_tiles"]
+    assert tiles > 0 and far > 0, (far, tiles)  # the far path ran
+    print(st, far / tiles)
 
 
 @pytest.mark.parametrize("launch", [(1, 4, 0), (2, 4, 3), (1, 2, 0), (2, 2, 3), (4, 2, 0),
@@ -51,12 +53,14 @@ def test_spatial_matches_oracle_and_address_order(gpu, order, delta):
 def test_spatial_launch_shapes(gpu, launch):
     """Every shape: the packed ones (two i per instruction) take far tiles,
     the one-i-per-thread ones only the Morton order of i and j."""
-    case = T.build_case(2, 3000, seed=22, binaries=0.1)
-    sel = np.random.default_rng(5).choice(3000, 2500, replace=False)
+    case = T.build_case(2, 6000, seed=22, binaries=0.1)
+    sel = np.random.default_rng(5).choice(6000, 5000, replace=False)
     want = T.oracle_force(case, sel=sel)
     got = T.run_library(case, sp.DOUBLESINGLE, sel=sel, launch=launch,
                         spatial=(EVERY_CALL, 1e-5))
     ref = T.run_library(case, sp.DOUBLESINGLE, sel=sel, launch=launch, spatial=(0, 0.0))
+    far, tiles = got["far_tiles"]
+    assert (far > 0) == (launch[1] > 1), (far, tiles)  # packed shapes only
     T.check_forces(got, want, 2)
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want, sel=sel)
     _same_neighbours(got, ref)
@@ -125,12 +129,34 @@ def test_spatial_forces_do_not_depend_on_h2(gpu):
     case = T.build_case(2, 6000, seed=27, binaries=0.1)
     wide = dict(case)
     wide["h2"] = np.full(case["n"], 0.15 ** 2)
-    a = T.run_library(case, sp.DOUBLESINGLE, spatial=(EVERY_CALL, 1e-5))
-    b = T.run_library(wide, sp.DOUBLESINGLE, spatial=(EVERY_CALL, 1e-5))
-    ref = T.run_library(wide, sp.DOUBLESINGLE, spatial=(0, 0.0))
+    a = T.run_library(case, sp.DOUBLESINGLE, launch=(1, 4, 0), spatial=(EVERY_CALL, 1e-5))
+    b = T.run_library(wide, sp.DOUBLESINGLE, launch=(1, 4, 0), spatial=(EVERY_CALL, 1e-5))
+    ref = T.run_library(wide, sp.DOUBLESINGLE, launch=(1, 4, 0), spatial=(0, 0.0))
+    assert b["far_tiles"][0] > 0
     assert np.array_equal(a["raw"], b["raw"])
     _same_neighbours(b, ref)
     assert np.mean(b["ngb_count"]) > 10  # lists reach far beyond the near tiles
+
+
+def test_spatial_grape5_order(gpu):
+    """GRAPE-5 order (acceleration and potential only, the self pair kept,
+    no neighbours) in spatial mode against the oracle; far tiles are taken."""
+    from oracle import oracle as O
+    case = T.build_case(1, 6000, seed=28, binaries=0.1)
+    n, eps2 = case["n"], 1e-6
+    x, m = case["x"], case["m"]
+    z = np.zeros((n, 3))
+    with sp.Sapporo(order=sp.GRAPE5, precision=sp.DOUBLESINGLE) as s:
+        s.set_launch(1, 4, 0)
+        s.set_spatial(EVERY_CALL, 1e-5)
+        s.set_j_particles(np.arange(n), case["id"], np.zeros(n), m, x, z, z, z)
+        s.start(n, case["id"], x, z, None, eps2, np.full(n, 1.0))
+        got = s.results(n)
+        far, tiles = s.spatial_stats()
+    want = O.force(1, x, z, None, np.zeros(n), np.full(n, -7, dtype=np.int32), x, z, None, m,
+                   case["id"], eps2, lists=False)
+    T.check_forces({"acc": got["acc"], "pot": got["pot"]}, want, 1, fields=["acc", "pot"])
+    assert tiles > 0 and far > tiles // 4, (far, tiles)
 
 
 def test_spatial_default_mode_threshold(gpu):
