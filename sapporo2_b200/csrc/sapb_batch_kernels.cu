@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
     if (item >= B.par->n_items) break;
     const BatchItem W = B.items[item];
     const float eps2f = (float)(B.cl[W.cluster].eps2 * (double)kTau);  // mixed pair: tau * eps2
-    const double eps2d = B.cl[W.cluster].eps2;
+    const double eps2d = B.cl[W.cluster].eps2 * kTau64;                 // FP64 pair: tau * eps2
     const int tpi = W.tpi;
     const int tit = kBT / tpi;
     const int tx = tid % tit;
@@ -237,6 +237,9 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
                      sc * t[5 * kBT], sc * t[6 * kBT], sc * t[7 * kBT], sc * t[8 * kBT],
                      sc * t[9 * kBT]};
       }
+    } else {  // FP64 sums of acc, jerk, snap carry -1/tau (kTau64)
+#pragma unroll
+      for (int p = 0; p < 2; p++) scale_dp(D[p], -kTau64);
     }
     // nearest neighbour: one rescan of the best tile (from L2)
     unsigned long long key[2];

@@ -17,6 +17,9 @@ namespace sapb {
 // when the totals are read.
 constexpr float kTau = 0x1.555556p-2f;        // fl32(1/3)
 constexpr double kSqrtTau = 0.5773502777928151;  // sqrt((double)kTau)
+// The FP64 pair does the same with tau = fl64(1/3).
+constexpr double kTau64 = 0x1.5555555555555p-2;     // fl64(1/3)
+constexpr double kSqrtTau64 = 0.5773502691896257;  // sqrt(kTau64), rounded
 
 // Force record of one predicted j (see sapb_internal.cuh for the layouts).
 template <int ORDER, int PREC>
@@ -25,7 +28,7 @@ __device__ __forceinline__ void store_record(void *pred, int k, double px, doubl
                                              double ax, double ay, double az) {
   if (PREC == DOUBLE) {
     double4 *r = reinterpret_cast<double4 *>(pred) + (size_t)k * pred_fields64(ORDER);
-    r[0] = make_double4(px, py, pz, m);
+    r[0] = make_double4(px, py, pz, m * kSqrtTau64);  // scaled mass (kTau64 above)
     r[1] = make_double4(vx, vy, vz, __hiloint2double(0, id));
     if (ORDER >= SIXTH) r[2] = make_double4(ax, ay, az, 0.0);
   } else {
@@ -357,17 +360,18 @@ __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const d
   double dx, dy, dz;
   const double ds2 = pair_dr_dp(I, r0, r1, dx, dy, dz);
   tmin = fmin(tmin, ds2);
-  const double inv = rsqrt(ds2 + eps2);
-  const double inv2 = inv * inv;
-  const double minv = r0.w * inv;
-  const double minv3 = minv * inv2;
+  // scaled rsqrt (kTau64 above; eps2 here is tau * eps2): y^2 = 3/r^2
+  const double y = rsqrt(fma(ds2, kTau64, eps2));
+  const double k = -(y * y);       // -3/r^2
+  const double minv = r0.w * y;    // m/r
+  const double minv3 = minv * k;   // -3 m/r^3: acc, jerk, snap carry -1/tau
   A.ax = fma(minv3, dx, A.ax);
   A.ay = fma(minv3, dy, A.ay);
   A.az = fma(minv3, dz, A.az);
   A.pot -= minv;
   const double dvx = r1.x - I.vx, dvy = r1.y - I.vy, dvz = r1.z - I.vz;
   const double rv = fma(dz, dvz, fma(dy, dvy, dx * dvx));
-  const double m3i2 = -3.0 * inv2;
+  const double m3i2 = k;
   const double a3 = m3i2 * rv;
   if (ORDER == FOURTH) {
     A.jx = fma(minv3, fma(a3, dx, dvx), A.jx);
@@ -386,6 +390,13 @@ __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const d
     A.sy = fma(minv3, fma(a6, ty, fma(b3, dy, day)), A.sy);
     A.sz = fma(minv3, fma(a6, tz, fma(b3, dz, daz)), A.sz);
   }
+}
+
+// Acceleration, jerk and snap of an FP64 sum times sc (the potential stays).
+__device__ __forceinline__ void scale_dp(AccDp &D, double sc) {
+  D.ax *= sc; D.ay *= sc; D.az *= sc;
+  D.jx *= sc; D.jy *= sc; D.jz *= sc;
+  D.sx *= sc; D.sy *= sc; D.sz *= sc;
 }
 
 __device__ __forceinline__ void list_push(int *cnt, int *list, int gi, int idj) {
