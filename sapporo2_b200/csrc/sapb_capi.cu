@@ -517,9 +517,11 @@ double *sapb_i_stage(sapb_dev *d, int ni) {
   return d->irec_h;
 }
 
-// Spatial mode pays for its orderings (a few sorts, ~0.1 ms at 2^20) once a
-// call has this many pairs; below it the calls run in address order.
-constexpr double kSpatialMinPairs = 268435456.0;  // 2^28
+// Spatial mode pays for its per-call work (the i sort and bounds, the j
+// gather after each prediction) from about 2^30 pairs on (B200, predict +
+// force per call: 0.99-1.03 x at 2^30, 1.03-1.04 x at 2^31, 1.08 x at 2^33 and
+// above); calls below this many pairs run in address order.
+constexpr double kSpatialMinPairs = 2147483648.0;  // 2^31
 
 static bool use_spatial(const sapb_dev *d, int ni, int nj) {
   if (d->prec != DOUBLESINGLE || d->sp.mode == 0) return false;

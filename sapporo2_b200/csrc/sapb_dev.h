@@ -24,6 +24,7 @@ struct SpatialBufs {
   int jcap = 0, icap = 0;
   int valid_nj = -1;          // j count of the current ordering (-1: none)
   unsigned long long valid_gen = 0;  // pred_gen it was built from
+  int order_age = 0;          // gathers with the current order since it was made
 };
 
 struct sapb_dev {

@@ -11,7 +11,9 @@
 // with the 3-operation difference (pair_mix2_far).
 //
 // Per force call in spatial mode:
-//   j (once per change of the predicted records):
+//   j (once per change of the predicted records; the first three steps only
+//   for a new j count and after every 16 changes, otherwise the previous
+//   order is reused):
 //     frame_kernel   bounding box of the j high parts (ordered-int atomics)
 //     jkey_kernel    30-bit Morton key of every j record in that box
 //     radix sort     (key, record) pairs, CUB
@@ -318,10 +320,22 @@ static cudaError_t ensure_i(SpatialBufs &S, int ni) {
   return cudaSuccess;
 }
 
+// Full ordering (full != 0): bounding box, keys, sort, then the gather.
+// Otherwise only the gather, with the previous call's order and keys: the
+// records are in the order of their positions some predictions ago, each
+// tile's box is recomputed from the current positions (so the far test stays
+// exact), and the first keys, which only pick the tile the nearest-neighbour
+// bound is taken over, stay valid as an order.
 template <int RS>
-static cudaError_t sort_j(sapb_dev *d, int nj, cudaStream_t st) {
+static cudaError_t order_j(sapb_dev *d, int nj, bool full, cudaStream_t st) {
   SpatialBufs &S = d->sp;
   const float4 *pred = static_cast<const float4 *>(d->pred);
+  const int tiles = (nj + kTJ - 1) / kTJ;
+  if (!full) {
+    gather_kernel<RS><<<tiles, kTJ, 0, st>>>(pred, S.jidx[1], S.jkey[1], nj,
+                                             static_cast<float4 *>(S.spred), S.tbox, S.tkey);
+    return cudaGetLastError();
+  }
   frame_init_kernel<<<1, 32, 0, st>>>(S.frame);
   const int blocks = std::min((nj + 255) / 256, std::max(d->num_sms, 1) * 8);
   frame_kernel<RS><<<blocks, 256, 0, st>>>(pred, nj, S.frame);
@@ -332,11 +346,15 @@ static cudaError_t sort_j(sapb_dev *d, int nj, cudaStream_t st) {
   e = cub::DeviceRadixSort::SortPairs(S.temp, tb, S.jkey[0], S.jkey[1], S.jidx[0], S.jidx[1], nj,
                                       0, 30, st);
   if (e != cudaSuccess) return e;
-  const int tiles = (nj + kTJ - 1) / kTJ;
   gather_kernel<RS><<<tiles, kTJ, 0, st>>>(pred, S.jidx[1], S.jkey[1], nj,
                                            static_cast<float4 *>(S.spred), S.tbox, S.tkey);
   return cudaGetLastError();
 }
+
+// Gathers with a previous order between two full orderings: the predicted
+// records change every block step, while particles cross a Morton cell
+// (~1/1000 of the cluster) in many steps.
+constexpr int kReorderEvery = 16;
 
 int spatial_prepare(sapb_dev *d, int nj, int ni, const double *i_dev) {
   SpatialBufs &S = d->sp;
@@ -350,7 +368,10 @@ int spatial_prepare(sapb_dev *d, int nj, int ni, const double *i_dev) {
     return sapb_fail(d, SAPB_ENOMEM, "spatial ordering buffers: %s", cudaGetErrorString(e));
   }
   if (S.valid_nj != nj || d->pred_gen != S.valid_gen) {
-    e = rs == 4 ? sort_j<4>(d, nj, st) : sort_j<3>(d, nj, st);
+    // a new order when the j count changed or after kReorderEvery reuses
+    const bool full = S.valid_nj != nj || S.order_age >= kReorderEvery;
+    S.order_age = full ? 0 : S.order_age + 1;
+    e = rs == 4 ? order_j<4>(d, nj, full, st) : order_j<3>(d, nj, full, st);
     if (e != cudaSuccess)
       return sapb_fail(d, SAPB_ECUDA, "spatial ordering of j: %s", cudaGetErrorString(e));
     S.valid_nj = nj;
