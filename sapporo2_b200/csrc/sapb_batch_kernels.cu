@@ -80,8 +80,8 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
     const int item = s_item;
     if (item >= B.par->n_items) break;
     const BatchItem W = B.items[item];
-    const float eps2f = (float)(B.cl[W.cluster].eps2 * (double)kTau);  // mixed pair: tau * eps2
-    const double eps2d = B.cl[W.cluster].eps2 * kTau64;                 // FP64 pair: tau * eps2
+    const float eps2f = (float)B.cl[W.cluster].eps2;
+    const double eps2d = B.cl[W.cluster].eps2;
     const int tpi = W.tpi;
     const int tit = kBT / tpi;
     const int tx = tid % tit;
@@ -228,18 +228,13 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
     }
     tbase += nt;
 
-    if (PREC != DOUBLE) {  // mixed sums of acc, jerk, snap carry -1/tau (kTau)
-      const double sc = -(double)kTau;
+    if (PREC != DOUBLE) {
 #pragma unroll
       for (int p = 0; p < 2; p++) {
         const double *t = tot + (size_t)p * 10 * kBT + tid;
-        D[p] = AccDp{sc * t[0], sc * t[kBT], sc * t[2 * kBT], t[3 * kBT], sc * t[4 * kBT],
-                     sc * t[5 * kBT], sc * t[6 * kBT], sc * t[7 * kBT], sc * t[8 * kBT],
-                     sc * t[9 * kBT]};
+        D[p] = AccDp{t[0], t[kBT], t[2 * kBT], t[3 * kBT], t[4 * kBT], t[5 * kBT], t[6 * kBT],
+                     t[7 * kBT], t[8 * kBT], t[9 * kBT]};
       }
-    } else {  // FP64 sums of acc, jerk, snap carry -1/tau (kTau64)
-#pragma unroll
-      for (int p = 0; p < 2; p++) scale_dp(D[p], -kTau64);
     }
     // nearest neighbour: one rescan of the best tile (from L2)
     unsigned long long key[2];

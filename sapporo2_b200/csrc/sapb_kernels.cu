@@ -233,8 +233,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 #pragma unroll
     for (int q = 0; q < IP * 10; q++) tot[q * kBT + tid] = 0.0;
   }
-  const float eps2f = (float)(A.eps2 * (double)kTau);  // mixed pair: tau * eps2
-  const double eps2d = A.eps2 * kTau64;                // FP64 pair: tau * eps2
+  const float eps2f = (float)A.eps2;
   const float2 eps2v = make_float2(eps2f, eps2f);
   constexpr int NPAIR = IP / 2;  // packed i pairs per thread (mixed precision)
   IMix2 I2[NPAIR > 0 ? NPAIR : 1];
@@ -286,7 +285,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
         const double4 r1 = rec[k * C::RS + 1];
         const double4 r2 = ORDER >= SIXTH ? rec[k * C::RS + 2] : r1;
 #pragma unroll
-        for (int p = 0; p < IP; p++) pair_dp<ORDER>(Id[p], r0, r1, r2, eps2d, D[p], tmin[p]);
+        for (int p = 0; p < IP; p++) pair_dp<ORDER>(Id[p], r0, r1, r2, A.eps2, D[p], tmin[p]);
       }
 #pragma unroll
       for (int p = 0; p < IP; p++) {
@@ -442,18 +441,13 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
       mbar_wait_bounded(&full[it % C::NS], (uint32_t)((it / C::NS) & 1));
   }
 
-  if (PREC != DOUBLE) {  // mixed sums of acc, jerk, snap carry -1/tau (kTau)
-    const double sc = -(double)kTau;
+  if (PREC != DOUBLE) {
 #pragma unroll
     for (int p = 0; p < IP; p++) {
       const double *t = tot + (size_t)p * 10 * kBT + tid;
-      D[p] = AccDp{sc * t[0], sc * t[kBT], sc * t[2 * kBT], t[3 * kBT], sc * t[4 * kBT],
-                   sc * t[5 * kBT], sc * t[6 * kBT], sc * t[7 * kBT], sc * t[8 * kBT],
-                   sc * t[9 * kBT]};
+      D[p] = AccDp{t[0], t[kBT], t[2 * kBT], t[3 * kBT], t[4 * kBT], t[5 * kBT], t[6 * kBT],
+                   t[7 * kBT], t[8 * kBT], t[9 * kBT]};
     }
-  } else {  // FP64 sums of acc, jerk, snap carry -1/tau (kTau64)
-#pragma unroll
-    for (int p = 0; p < IP; p++) scale_dp(D[p], -kTau64);
   }
 
   // ---- nearest neighbour: one rescan of the best tile (from L2) ----

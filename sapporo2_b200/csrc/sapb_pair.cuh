@@ -8,19 +8,6 @@
 
 namespace sapb {
 
-// Scaled rsqrt of the mixed-precision pair (saves one FMA-pipe operation per
-// pair): y = rsqrt(tau (r^2 + eps2)) with tau = fl32(1/3) gives y^2 = 3/r^2
-// (to 3e-8), so k = -y^2 serves both as the 1/r^2 of m/r^3 and as the -3/r^2
-// of the jerk and snap coefficients.  The record carries m sqrt(tau), so
-// m_rec y = m/r exactly as before (potential unchanged); acceleration, jerk
-// and snap come out multiplied by -1/tau and are scaled back by -tau in FP64
-// when the totals are read.
-constexpr float kTau = 0x1.555556p-2f;        // fl32(1/3)
-constexpr double kSqrtTau = 0.5773502777928151;  // sqrt((double)kTau)
-// The FP64 pair does the same with tau = fl64(1/3).
-constexpr double kTau64 = 0x1.5555555555555p-2;     // fl64(1/3)
-constexpr double kSqrtTau64 = 0.5773502691896257;  // sqrt(kTau64), rounded
-
 // Force record of one predicted j (see sapb_internal.cuh for the layouts).
 template <int ORDER, int PREC>
 __device__ __forceinline__ void store_record(void *pred, int k, double px, double py, double pz,
@@ -28,7 +15,7 @@ __device__ __forceinline__ void store_record(void *pred, int k, double px, doubl
                                              double ax, double ay, double az) {
   if (PREC == DOUBLE) {
     double4 *r = reinterpret_cast<double4 *>(pred) + (size_t)k * pred_fields64(ORDER);
-    r[0] = make_double4(px, py, pz, m * kSqrtTau64);  // scaled mass (kTau64 above)
+    r[0] = make_double4(px, py, pz, m);
     r[1] = make_double4(vx, vy, vz, __hiloint2double(0, id));
     if (ORDER >= SIXTH) r[2] = make_double4(ax, ay, az, 0.0);
   } else {
@@ -38,7 +25,7 @@ __device__ __forceinline__ void store_record(void *pred, int k, double px, doubl
     const float lx = (float)(px - (double)hx), ly = (float)(py - (double)hy),
                 lz = (float)(pz - (double)hz);
     float4 *r = reinterpret_cast<float4 *>(pred) + (size_t)k * pred_fields(ORDER);
-    r[0] = make_float4(hx, hy, hz, (float)(m * kSqrtTau));  // scaled mass (kTau above)
+    r[0] = make_float4(hx, hy, hz, (float)m);
     r[1] = make_float4(lx, ly, lz, __int_as_float(id));
     r[2] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
     if (ORDER >= SIXTH) r[3] = make_float4((float)ax, (float)ay, (float)az, 0.f);
@@ -143,11 +130,10 @@ __device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const 
     ds2 = pair_dr_mix(I, r0, r1, dx, dy, dz);
     tmin = fminf(tmin, ds2);
   }
-  // eps2 here is tau * eps2 (scaled rsqrt, kTau above)
-  const float y = rsqrt_mufu(fmaf(ds2, kTau, eps2));
-  const float k = -(y * y);        // -3/r^2
-  const float minv = r0.w * y;     // m/r
-  const float minv3 = minv * k;    // -3 m/r^3: acc, jerk, snap carry -1/tau
+  const float inv = rsqrt_mufu(ds2 + eps2);
+  const float inv2 = inv * inv;
+  const float minv = r0.w * inv;
+  const float minv3 = minv * inv2;
   A.ax = fmaf(minv3, dx, A.ax);
   A.ay = fmaf(minv3, dy, A.ay);
   A.az = fmaf(minv3, dz, A.az);
@@ -155,7 +141,7 @@ __device__ __forceinline__ void pair_mix(const IMix &I, const float4 &r0, const 
   if (ORDER == GRAPE5) return;  // acceleration and potential only
   const float dvx = r2.x - I.vx, dvy = r2.y - I.vy, dvz = r2.z - I.vz;
   const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
-  const float m3i2 = k;
+  const float m3i2 = -3.0f * inv2;
   if (ORDER == FOURTH) {
     // jerk += m/r^3 (dv - 3 (dr.dv)/r^2 dr)   (kernels.cu:631-637)
     const float a3 = m3i2 * rv;
@@ -198,11 +184,6 @@ struct AccMix2 {
 
 __device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float2 neg2(float a, float b) { return make_float2(-a, -b); }
-// Sign flip by integer XOR: ALU pipe, not the FMA pipe the pair is bound by.
-__device__ __forceinline__ float2 neg2_alu(float2 a) {
-  return make_float2(__int_as_float(__float_as_int(a.x) ^ (int)0x80000000),
-                     __int_as_float(__float_as_int(a.y) ^ (int)0x80000000));
-}
 
 __device__ __forceinline__ IMix2 pack_i2(const IMix &a, const IMix &b) {
   IMix2 I;
@@ -245,7 +226,7 @@ __device__ __forceinline__ Pre2 pair_mix2_pre(const IMix2 &I, const float4 &r0, 
     tmin.x = fminf(tmin.x, ds2.x);
     tmin.y = fminf(tmin.y, ds2.y);
   }
-  const float2 r2v = __ffma2_rn(ds2, bc2(kTau), eps2);  // tau (r^2 + eps2)
+  const float2 r2v = __fadd2_rn(ds2, eps2);
   P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
   return P;
 }
@@ -254,11 +235,10 @@ template <int ORDER>
 __device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, float mj,
                                                const float4 &r2, const float4 &r3,
                                                AccMix2 &A) {
-  // scaled rsqrt (kTau above): y^2 = 3/r^2, mj = m sqrt(tau)
-  const float2 dx = P.dx, dy = P.dy, dz = P.dz, y = P.inv;
-  const float2 k = __fmul2_rn(y, neg2_alu(y));  // -3/r^2
-  const float2 minv = __fmul2_rn(bc2(mj), y);   // m/r
-  const float2 minv3 = __fmul2_rn(minv, k);     // -3 m/r^3: acc, jerk, snap carry -1/tau
+  const float2 dx = P.dx, dy = P.dy, dz = P.dz, inv = P.inv;
+  const float2 inv2 = __fmul2_rn(inv, inv);
+  const float2 minv = __fmul2_rn(bc2(mj), inv);
+  const float2 minv3 = __fmul2_rn(minv, inv2);
   A.ax = __ffma2_rn(minv3, dx, A.ax);
   A.ay = __ffma2_rn(minv3, dy, A.ay);
   A.az = __ffma2_rn(minv3, dz, A.az);
@@ -268,7 +248,7 @@ __device__ __forceinline__ void pair_mix2_post(const IMix2 &I, const Pre2 &P, fl
   const float2 dvy = __fadd2_rn(bc2(r2.y), I.nvy);
   const float2 dvz = __fadd2_rn(bc2(r2.z), I.nvz);
   const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
-  const float2 m3i2 = k;
+  const float2 m3i2 = __fmul2_rn(bc2(-3.0f), inv2);
   if (ORDER == FOURTH) {
     const float2 a3 = __fmul2_rn(m3i2, rv);
     A.jx = __ffma2_rn(minv3, __ffma2_rn(a3, dx, dvx), A.jx);
@@ -328,7 +308,7 @@ __device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, 
     tmin.x = fminf(tmin.x, ds2.x);
     tmin.y = fminf(tmin.y, ds2.y);
   }
-  const float2 r2v = __ffma2_rn(ds2, bc2(kTau), eps2);  // tau (r^2 + eps2)
+  const float2 r2v = __fadd2_rn(ds2, eps2);
   P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
   pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
@@ -360,18 +340,17 @@ __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const d
   double dx, dy, dz;
   const double ds2 = pair_dr_dp(I, r0, r1, dx, dy, dz);
   tmin = fmin(tmin, ds2);
-  // scaled rsqrt (kTau64 above; eps2 here is tau * eps2): y^2 = 3/r^2
-  const double y = rsqrt(fma(ds2, kTau64, eps2));
-  const double k = -(y * y);       // -3/r^2
-  const double minv = r0.w * y;    // m/r
-  const double minv3 = minv * k;   // -3 m/r^3: acc, jerk, snap carry -1/tau
+  const double inv = rsqrt(ds2 + eps2);
+  const double inv2 = inv * inv;
+  const double minv = r0.w * inv;
+  const double minv3 = minv * inv2;
   A.ax = fma(minv3, dx, A.ax);
   A.ay = fma(minv3, dy, A.ay);
   A.az = fma(minv3, dz, A.az);
   A.pot -= minv;
   const double dvx = r1.x - I.vx, dvy = r1.y - I.vy, dvz = r1.z - I.vz;
   const double rv = fma(dz, dvz, fma(dy, dvy, dx * dvx));
-  const double m3i2 = k;
+  const double m3i2 = -3.0 * inv2;
   const double a3 = m3i2 * rv;
   if (ORDER == FOURTH) {
     A.jx = fma(minv3, fma(a3, dx, dvx), A.jx);
@@ -390,13 +369,6 @@ __device__ __forceinline__ void pair_dp(const IDp &I, const double4 &r0, const d
     A.sy = fma(minv3, fma(a6, ty, fma(b3, dy, day)), A.sy);
     A.sz = fma(minv3, fma(a6, tz, fma(b3, dz, daz)), A.sz);
   }
-}
-
-// Acceleration, jerk and snap of an FP64 sum times sc (the potential stays).
-__device__ __forceinline__ void scale_dp(AccDp &D, double sc) {
-  D.ax *= sc; D.ay *= sc; D.az *= sc;
-  D.jx *= sc; D.jy *= sc; D.jz *= sc;
-  D.sx *= sc; D.sy *= sc; D.sz *= sc;
 }
 
 __device__ __forceinline__ void list_push(int *cnt, int *list, int gi, int idj) {
