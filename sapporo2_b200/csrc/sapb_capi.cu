@@ -518,15 +518,17 @@ double *sapb_i_stage(sapb_dev *d, int ni) {
 }
 
 // Spatial mode pays for its per-call work (the i sort and bounds, the j
-// gather after each prediction) from about 2^30 pairs on (B200, predict +
-// force per call: 0.99-1.03 x at 2^30, 1.03-1.04 x at 2^31, 1.08 x at 2^33 and
-// above); calls below this many pairs run in address order.
-constexpr double kSpatialMinPairs = 2147483648.0;  // 2^31
+// gather after each prediction) from about 2^29 pairs and 2048 i on (B200,
+// predict + force per call, i a random subset of the j: 1.00-1.03 x from 2^29
+// to 2^31, 1.06-1.08 x from 2^33; block-step active sets, which are spatially
+// clustered, gain more); smaller calls run in address order.
+constexpr double kSpatialMinPairs = 536870912.0;  // 2^29
+constexpr int kSpatialMinI = 2048;
 
 static bool use_spatial(const sapb_dev *d, int ni, int nj) {
   if (d->prec != DOUBLESINGLE || d->sp.mode == 0) return false;
   if (d->sp.mode == 2) return true;
-  return ni >= 1024 && nj >= 4 * force_tile_j() && (double)ni * nj >= kSpatialMinPairs;
+  return ni >= kSpatialMinI && nj >= 4 * force_tile_j() && (double)ni * nj >= kSpatialMinPairs;
 }
 
 static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
