@@ -197,14 +197,19 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
     far_tiles, warp_tiles = s.spatial_stats(reset=True)
     s.close()
     spatial = precision == sp.DOUBLESINGLE and spatial_on(n, nj)
-    # own kernels per step: predictor, force (+ slice reduction); in spatial
-    # mode the orderings add frame init, frame, j keys, gather, i keys and
-    # seeds (the two radix sorts are CUB's kernels, listed apart)
+    # own kernels in the timed steps: predictor, force (+ slice reduction);
+    # in spatial mode the j gather, i keys and bounds every step, plus frame
+    # init, frame and j keys on the steps that re-sort j (the first call and
+    # every 17th after it: the library reuses an order 16 times); the radix
+    # sorts are CUB's kernels, not counted
+    per = 2 + (1 if ns > 1 else 0) + (3 if spatial else 0)
+    timed = range(warmup, warmup + steps)
+    launches = per * steps + (3 * sum(1 for c in timed if c % 17 == 0) if spatial else 0)
     return {"pred_ms": pred_ms, "force_ms": force_ms, "comb_ms": comb_ms, "res": out,
             "plan": {"tpi": tpi, "ip": ip, "nslices": ns}, "nj_local": nj,
             "spatial": spatial,
             "far_fraction": far_tiles / warp_tiles if warp_tiles else None,
-            "launches_per_step": 2 + (1 if ns > 1 else 0) + (6 if spatial else 0)}
+            "launches": launches}
 
 
 def e2e_arm(cfg, steps: int, shard=None):
@@ -738,7 +743,7 @@ def main():
                 "s_per_step": e2e["s_per_step"], "api": "sapporo class, n_pipes chunks",
                 "chunks": e2e["chunks"]},
         "clocks": clk,
-        "gpu_launches": mix["launches_per_step"] * args.steps,
+        "gpu_launches": mix["launches"],
     }
     # accuracy: mixed vs all-FP64 GPU kernel on all N
     rm, rd = mix["res"], f64["res"]
