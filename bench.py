@@ -415,6 +415,72 @@ def run_learned_h2_bench(args):
     }), flush=True)
 
 
+def run_spatial_sizes_bench(args, torch):
+    """Where the spatial mode pays: one call = prediction of all j + force
+    on ni i (a random subset of the j, 6th order, mixed, lists on), timed on
+    the device (median of the timed calls), with the spatial mode off (0)
+    and on for every call (2); j = 131072 and 2^20 Plummer + 10 % binaries."""
+    import sapporo2_b200 as sp
+    from sapporo2_b200 import ic
+    sizes = [512, 1024, 2048, 4096, 8192, 16384, 65536]
+    rows = []
+    for nj in (131072, 1 << 20):
+        cfg = ic.make_config("C3", n=nj, seed=3)
+        rng = np.random.default_rng(1)
+        z = np.zeros((nj, 3))
+        sels = {ni: np.sort(rng.choice(nj, ni, replace=False)) for ni in sizes}
+        ms = {}
+        for mode in (0, 2):
+            s = sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE)
+            s.set_spatial(mode, 0.0)
+            stream = torch.cuda.Stream()
+            s.set_stream(stream.cuda_stream)
+            s.set_j_particles(np.arange(nj), cfg["id"], np.zeros(nj), cfg["m"], cfg["x"],
+                              cfg["v"], z, z, z, z)
+            s.force_prediction(nj)
+            lib, dev = s.lib, s.dev
+            for ni in sizes:
+                sel = sels[ni]
+                rec = sp.pack_i_records(2, cfg["x"][sel], cfg["v"][sel], np.full(ni, 1e-4),
+                                        cfg["id"][sel], z[sel])
+                i_dev = torch.from_numpy(rec).cuda()
+                res = torch.zeros((ni, sp.RES_STRIDE), dtype=torch.float64, device="cuda")
+                cnt = torch.zeros(ni, dtype=torch.int32, device="cuda")
+                lst = torch.zeros(ni * sp.NGB_PB, dtype=torch.int32, device="cuda")
+                ts = []
+                for it in range(args.warmup + args.steps):
+                    e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+                    e0.record(stream)
+                    rc = lib.sapb_predict(dev, nj, 0.0)
+                    rc |= lib.sapb_force_device(dev, nj, ni, i_dev.data_ptr(), 1e-6,
+                                                sp.F_NGB_LIST, res.data_ptr(), cnt.data_ptr(),
+                                                lst.data_ptr())
+                    e1.record(stream)
+                    e1.synchronize()
+                    if rc:
+                        raise RuntimeError(lib.sapb_last_error(dev).decode())
+                    if it >= args.warmup:
+                        ts.append(e0.elapsed_time(e1))
+                ms[(mode, ni)] = float(np.median(ts))
+            s.set_stream(None)
+            s.close()
+        for ni in sizes:
+            a, b = ms[(0, ni)], ms[(2, ni)]
+            rows.append({"nj": nj, "ni": ni, "log2_pairs": round(float(np.log2(ni * nj)), 1),
+                         "address_ms": a, "spatial_ms": b, "speedup": a / b})
+            log(f"[bench] nj {nj} ni {ni}: address {a:.3f} ms spatial {b:.3f} ms x{a / b:.3f}")
+    big = [r["speedup"] for r in rows if r["log2_pairs"] >= 33]
+    print(json.dumps({
+        "metric": "spatial mode / address order speed-up per call (predict + force, 6th order, "
+                  "mixed, lists on), calls of >= 2^33 pairs",
+        "value": float(np.mean(big)), "unit": "x", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 body + ds positions (near tiles) + f64 sums", "data": "synthetic",
+        "config": {"workload": "call sizes: i random subsets of j = 131072 and 2^20 (Plummer + "
+                               "10 % binaries)", "rows": rows},
+    }), flush=True)
+
+
 def run_blocksteps_bench(args):
     """Block time steps of one system (N = 131072 Plummer, 6th order,
     dt = 2^-k with k uniform in 3..12, lists on with h2 for ~32 neighbours):
@@ -556,11 +622,14 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2", "blocksteps"],
+    ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2", "blocksteps",
+                                           "spatial_sizes"],
                     default="precision",
                     help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters; "
                          "learned_h2: block steps with fixed, count-scaled and learned h2; "
-                         "blocksteps: block steps of one system, class vs batch API")
+                         "blocksteps: block steps of one system, class vs batch API; "
+                         "spatial_sizes: predict + force per call, address order vs spatial "
+                         "mode, over call sizes")
     ap.add_argument("--bs-steps", type=int, default=64)
     ap.add_argument("--multi", choices=["shard", "replicas"], default="shard",
                     help="N>1 GPUs: shard: one N-body system, j split over the ranks "
@@ -609,6 +678,9 @@ def main():
         return
     if args.workload == "blocksteps":
         run_blocksteps_bench(args)
+        return
+    if args.workload == "spatial_sizes":
+        run_spatial_sizes_bench(args, torch)
         return
     n = args.n
     sharded = world > 1 and args.multi == "shard"
