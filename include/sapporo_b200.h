@@ -260,6 +260,20 @@ int sapb_set_spatial(sapb_dev *d, int mode, double delta);
 int sapb_spatial_stats(sapb_dev *d, unsigned long long *far_tiles,
                        unsigned long long *warp_tiles, int reset);
 
+/* Near pairs of the mixed-precision (DOUBLESINGLE) force calls, an addition
+ * to the reference's double-single kernels (kernels.cu:552-669, which take
+ * every pair in FP32 after the position difference): when an i's share of a
+ * j tile holds a pair with ds2 < factor * eps2, that share is summed in FP64
+ * instead (positions hi + lo, velocity, acceleration and mass as stored).
+ * Softened pairs a few softening lengths apart can dominate an i's jerk or
+ * snap while their sum passes through zero, and there FP32 rounding would
+ * leave large relative errors; tight binaries are such pairs.  factor 0 turns
+ * it off (every pair in FP32, as the reference); the default is 16 (pairs
+ * within 4 softening lengths).  The environment variable SAPPORO_B200_NEAR
+ * sets the factor at open.  No effect with eps2 = 0 or on the FP64 and
+ * GRAPE-5 kernels.  Batch calls take every pair in FP32. */
+int sapb_set_near(sapb_dev *d, double factor);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,7 @@ _SIGS = [
     ("sapb_set_spatial", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     ("sapb_spatial_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong),
                                      C.POINTER(C.c_ulonglong), C.c_int]),
+    ("sapb_set_near", C.c_int, [C.c_void_p, C.c_double]),
     ("sapb_get_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 3),
     ("sapb_batch_create", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     ("sapb_batch_destroy", C.c_int, [C.c_void_p]),
@@ -396,6 +397,11 @@ class Sapporo:
         single-float difference, accurate to `delta` (0: 1e-6)."""
         _check(self.lib.sapb_set_spatial(self.dev, int(mode), float(delta)), "set_spatial",
                self.dev)
+
+    def set_near(self, factor=16.0):
+        """Mixed precision: an i's share of a j tile holding a pair with
+        ds2 < factor * eps2 is summed in FP64 (0: every pair in FP32)."""
+        _check(self.lib.sapb_set_near(self.dev, float(factor)), "set_near", self.dev)
 
     def spatial_stats(self, reset=False):
         """(far, all) (warp, j tile) pairs of the spatial-mode calls since the

@@ -74,6 +74,9 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
 
   int tbase = 0;  // tiles this block has streamed so far (ring position)
   bool broken = false;
+  // thread 0: ring positions issued / seen arrived; after a timed-out wait
+  // the copies in between are drained before the block exits
+  int n_issued = 0, n_landed = 0;
   for (;;) {
     if (tid == 0) s_item = atomicAdd(&B.par->queue_head, 1);
     __syncthreads();
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
       const int st = T % kNS;
       const int cnt = min(kTJ, W.j_count - t * kTJ);
       const uint32_t bytes = (uint32_t)(cnt * C::REC);
+      n_issued = T + 1;
       fence_proxy_async();
       mbar_expect_tx(&full[st], bytes);
       bulk_g2s(tiles + st * C::TILE_BYTES, pred + (size_t)(W.j_begin + t * kTJ) * C::REC, bytes,
@@ -156,9 +160,13 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
     for (int it = 0; it < nt; it++) {
       const int T = tbase + it;
       const int s = T % kNS;
-      if (!broken && !mbar_wait_bounded(&full[s], (uint32_t)((T / kNS) & 1))) {
-        broken = true;
-        atomicOr(B.status, kErrWaitTimeout);
+      if (!broken) {
+        if (mbar_wait_bounded(&full[s], (uint32_t)((T / kNS) & 1))) {
+          n_landed = T + 1;
+        } else {
+          broken = true;
+          atomicOr(B.status, kErrWaitTimeout);
+        }
       }
       const int cnt = min(kTJ, W.j_count - it * kTJ);
       const unsigned char *buf = tiles + s * C::TILE_BYTES;
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
     }
   }
   if (broken && tid == 0) {
-    for (int T = max(tbase - kNS, 0); T < tbase; T++)
+    for (int T = n_landed; T < n_issued; T++)
       mbar_wait_bounded(&full[T % kNS], (uint32_t)((T / kNS) & 1));
   }
 }

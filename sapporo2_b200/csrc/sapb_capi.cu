@@ -357,6 +357,10 @@ int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
   d->n_pipes = n_pipes > 0 ? n_pipes : SAPB_NPIPES;
   d->sp.far_c = (float)(0x1p-23 / kSpatialDelta);
   if (const char *e = getenv("SAPPORO_B200_SPATIAL")) d->sp.mode = atoi(e) == 0 ? 0 : (atoi(e) >= 2 ? 2 : 1);
+  if (const char *e = getenv("SAPPORO_B200_NEAR")) {
+    const double k = atof(e);
+    if (k >= 0.0 && k <= 1e6) d->near_k = k;
+  }
   int rc = SAPB_OK;
   do {
     if (cudaSetDevice(device) != cudaSuccess) { rc = fail(d, SAPB_ECUDA, "cudaSetDevice(%d)", device); break; }
@@ -531,6 +535,13 @@ static bool use_spatial(const sapb_dev *d, int ni, int nj) {
   return ni >= kSpatialMinI && nj >= 4 * force_tile_j() && (double)ni * nj >= kSpatialMinPairs;
 }
 
+// Near-pair radius^2 of a mixed-precision call (FP32, compared with the
+// kernels' double-single ds2); 0 turns the FP64 near-pair sums off.
+static float near_r2(const sapb_dev *d, double eps2) {
+  if (d->prec == DOUBLE || d->order == GRAPE5) return 0.0f;
+  return (float)(d->near_k * eps2);
+}
+
 static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double eps2, int flags,
                      double *res_dev, int *cnt_dev, int *list_dev) {
   if (nj <= 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "nj = %d (capacity %d)", nj, d->cap);
@@ -557,6 +568,7 @@ static int run_force(sapb_dev *d, int nj, int ni, const double *i_dev, double ep
   A.irec = i_dev;
   A.ni = ni;
   A.eps2 = eps2;
+  A.near_r2 = near_r2(d, eps2);
   A.nslices = P.ns;
   A.i_tiles = P.i_tiles;
   A.do_list = list ? 1 : 0;
@@ -673,9 +685,9 @@ int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, 
     return fail(d, SAPB_EINVAL,
                 "sapb_force_device_noalloc: ni = %d exceeds the fixed scratch (at most %zu "
                 "i-particles per call)", ni, cap_records);
-  if (nj <= 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "nj = %d (capacity %d)", nj, d->cap);
   CK(d, cudaSetDevice(d->device));
-  if (ni == 0) return SAPB_OK;
+  if (ni == 0) return SAPB_OK;  // as sapb_force_device: an empty call does nothing
+  if (nj <= 0 || nj > d->cap) return fail(d, SAPB_EINVAL, "nj = %d (capacity %d)", nj, d->cap);
   int rc = noalloc_setup(d);  // normally already done by sapb_open
   if (rc) return rc;
   double *scratch = g_noalloc_ptr[d->device];
@@ -697,6 +709,7 @@ int sapb_force_device_noalloc(sapb_dev *d, int nj, int ni, const double *i_dev, 
   A.irec = i_dev;
   A.ni = ni;
   A.eps2 = eps2;
+  A.near_r2 = near_r2(d, eps2);
   A.nslices = P.ns;
   A.i_tiles = P.i_tiles;
   A.do_list = list ? 1 : 0;
@@ -717,6 +730,14 @@ int sapb_set_spatial(sapb_dev *d, int mode, double delta) {
     return fail(d, SAPB_EINVAL, "spatial mode %d, delta %g (mode 0..2, delta 0..1e-4)", mode, delta);
   d->sp.mode = mode;
   d->sp.far_c = (float)(0x1p-23 / (delta > 0.0 ? delta : kSpatialDelta));
+  return SAPB_OK;
+}
+
+int sapb_set_near(sapb_dev *d, double factor) {
+  if (!d) return fail(nullptr, SAPB_EINVAL, "null device");
+  if (!(factor >= 0.0) || factor > 1e6)
+    return fail(d, SAPB_EINVAL, "near-pair factor %g (0..1e6)", factor);
+  d->near_k = factor;
   return SAPB_OK;
 }
 

@@ -65,6 +65,10 @@ struct sapb_dev {
   // launch overrides (0 = planner)
   int tpi = 0, ip = 0, nslices = 0;
 
+  // mixed precision: pairs with ds2 < near_k * eps2 are summed in FP64
+  // (0: every pair in FP32)
+  double near_k = 16.0;
+
   SpatialBufs sp;
 
   char err[512] = {0};

@@ -80,6 +80,9 @@ struct ForceArgs {
   const float4 *tbox;   // [2 * tiles]: {min xyz, max |x|}, {max xyz, 0} of the high parts
   float far_c;          // 2^-23 / delta: far tiles are >= far_c * |x|max from every i
   unsigned long long *stats;  // [2]: += far (warp, tile) pairs, += all (warp, tile) pairs
+  // Near pairs (mixed precision; 0: off): an i whose row of a tile holds a j
+  // with ds2 < near_r2 has that row summed again in FP64 instead of FP32.
+  float near_r2;
 };
 
 // ---- batched execution (block steps, ensembles of independent clusters) ----

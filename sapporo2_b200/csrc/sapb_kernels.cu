@@ -172,7 +172,12 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   __syncthreads();
 
   // ---- producer: lane 0 of warp 0 fills the ring ----
+  // n_issued / n_landed (thread 0): tiles issued so far / tiles whose
+  // arrival it has seen; after a timed-out wait the copies in between are
+  // drained before the block exits
+  int n_issued = 0, n_landed = 0;
   auto issue = [&](int it) {
+    n_issued = it + 1;
     const int st = it % C::NS;
     const int tile = slice + it * S;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
@@ -246,8 +251,9 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   // A tile is far when, for every i of the warp, (1) its distance to the
   // tile's box is at least far_c * max(|xi|, |xj|) (single-float difference
   // accurate to delta) and (2) its squared distance, less a 1e-4 margin,
-  // exceeds lim = an upper bound of its nearest-neighbour ds2: no pair of the
-  // tile can then be a nearest neighbour.  The warp votes, so the decision
+  // exceeds lim = the larger of an upper bound of its nearest-neighbour ds2
+  // and near_r2: no pair of the tile can then be a nearest neighbour or a
+  // near pair (FP64 rescan, below).  The warp votes, so the decision
   // is warp-uniform.  It does not depend on h2, so neither do the forces:
   // list members in far tiles are found by an exact rescan, triggered by the
   // tile's approximate ds2 minimum.
@@ -255,7 +261,9 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 #pragma unroll
   for (int p = 0; p < IP; p++) {
     lim[p] = -1.f;
-    if (spatial && ORDER != GRAPE5 && valid[p]) lim[p] = __ldg(A.ibound + gi[p]);
+    // a far tile must also hold no near pair (ds2 < near_r2)
+    if (spatial && ORDER != GRAPE5 && valid[p])
+      lim[p] = fmaxf(__ldg(A.ibound + gi[p]), A.near_r2);
   }
   // Margin of the far tests: a box distance from high parts, and a ds2 from
   // the single-float difference, are within 2 sqrt(3) delta (relative) of the
@@ -266,9 +274,13 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
 
   for (int it = 0; it < nt; it++) {
     const int s = it % C::NS;
-    if (!broken && !mbar_wait_bounded(&full[s], (uint32_t)((it / C::NS) & 1))) {
-      broken = true;
-      atomicOr(A.status, kErrWaitTimeout);
+    if (!broken) {
+      if (mbar_wait_bounded(&full[s], (uint32_t)((it / C::NS) & 1))) {
+        n_landed = it + 1;
+      } else {
+        broken = true;
+        atomicOr(A.status, kErrWaitTimeout);
+      }
     }
     const int tile = slice + it * S;
     const int cnt = min(kTJ, A.nj - tile * kTJ);
@@ -391,18 +403,28 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
       }
 #pragma unroll
       for (int p = 0; p < IP; p++) {
+        // a near pair in this row (never on a far tile): the row is summed
+        // again in FP64 below, so its FP32 partial is dropped
+        const bool nearp = ORDER != GRAPE5 && !far && valid[p] && tmin[p] < A.near_r2;
         double *t = tot + (size_t)p * 10 * kBT + tid;
-        t[0 * kBT] += (double)P[p].ax;
-        t[1 * kBT] += (double)P[p].ay;
-        t[2 * kBT] += (double)P[p].az;
-        t[3 * kBT] += (double)P[p].pot;
-        t[4 * kBT] += (double)P[p].jx;
-        t[5 * kBT] += (double)P[p].jy;
-        t[6 * kBT] += (double)P[p].jz;
-        if (ORDER >= SIXTH) {
-          t[7 * kBT] += (double)P[p].sx;
-          t[8 * kBT] += (double)P[p].sy;
-          t[9 * kBT] += (double)P[p].sz;
+        if (!nearp) {
+          t[0 * kBT] += (double)P[p].ax;
+          t[1 * kBT] += (double)P[p].ay;
+          t[2 * kBT] += (double)P[p].az;
+          t[3 * kBT] += (double)P[p].pot;
+          t[4 * kBT] += (double)P[p].jx;
+          t[5 * kBT] += (double)P[p].jy;
+          t[6 * kBT] += (double)P[p].jz;
+          if (ORDER >= SIXTH) {
+            t[7 * kBT] += (double)P[p].sx;
+            t[8 * kBT] += (double)P[p].sy;
+            t[9 * kBT] += (double)P[p].sz;
+          }
+        }
+        if (ORDER != GRAPE5) {
+          const unsigned nm = __ballot_sync(0xffffffffu, nearp);
+          if (nm)
+            near_rescan_mix<ORDER, C::RS, TPI>(nm, oi[p], ty, rec, cnt, lane, A.irec, A.eps2, t);
         }
         if (ORDER != GRAPE5) {  // GRAPE-5: no nearest neighbour, no lists
           // a far tile holds no nearest neighbour; its minimum is the
@@ -435,9 +457,10 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
     atomicAdd(A.stats, (unsigned long long)nfar);
     atomicAdd(A.stats + 1, (unsigned long long)nt);
   }
-  if (broken && tid == 0) {
-    // let copies still in flight land before shared memory is released
-    for (int it = max(nt - C::NS, 0); it < nt; it++)
+  if (broken && producer) {
+    // let the copies still in flight land (bounded waits) before the block
+    // exits and its shared memory is released
+    for (int it = n_landed; it < n_issued; it++)
       mbar_wait_bounded(&full[it % C::NS], (uint32_t)((it / C::NS) & 1));
   }
 

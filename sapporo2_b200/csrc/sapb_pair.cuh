@@ -408,6 +408,80 @@ __device__ __forceinline__ void list_rescan_mix(const IMix &I, bool want, int gi
   }
 }
 
+// Near-pair rescan (mixed precision).  A pair closer than a few softening
+// lengths can carry most of an i's jerk or snap while passing through zero
+// (the radial snap of a softened pair vanishes at r^2 = 1.5 eps^2), and there
+// the FP32 rounding of its terms, ~1e-7 of their size, becomes a large
+// relative error of the small total.  So when an i's row of a tile holds a j
+// with the exact double-single ds2 below near_r2, the caller drops that row's
+// FP32 partial sum for the i and this routine sums the same records again in
+// FP64: the warp splits the row's j, each lane evaluates pair_dp on the
+// record widened to double (the double-single position hi + lo is exact in
+// double; velocity, acceleration and mass as stored) against the i's own FP64
+// record, and the warp sum is added to that i's FP64 totals by its lane.
+// `nm` is the ballot of the lanes that asked; rare, so kept out of line.
+template <int ORDER, int RS, int TPI>
+__device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, const float4 *rec,
+                                             int cnt, int lane, const double *irec, double eps2,
+                                             double *tot) {
+  while (nm) {
+    const int src = __ffs(nm) - 1;
+    nm &= nm - 1;
+    const int soi = __shfl_sync(0xffffffffu, oi, src);
+    const int srow = __shfl_sync(0xffffffffu, row, src);
+    const double *r = irec + (size_t)soi * i_stride(ORDER);
+    IDp I;
+    I.x = r[0]; I.y = r[1]; I.z = r[2]; I.h2 = 0.0;
+    I.vx = r[4]; I.vy = r[5]; I.vz = r[6];
+    I.id = __double2loint(r[7]);
+    I.ax = I.ay = I.az = 0.0;
+    if (ORDER >= SIXTH) {
+      I.ax = r[8]; I.ay = r[9]; I.az = r[10];
+    }
+    AccDp S{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double tmin = DBL_MAX;
+    for (int k = srow + lane * TPI; k < cnt; k += 32 * TPI) {
+      const float4 q0 = rec[k * RS + 0], q1 = rec[k * RS + 1], q2 = rec[k * RS + 2];
+      const float4 q3 = ORDER >= SIXTH ? rec[k * RS + 3] : q2;
+      const double4 j0 = make_double4((double)q0.x + (double)q1.x, (double)q0.y + (double)q1.y,
+                                      (double)q0.z + (double)q1.z, (double)q0.w);
+      const double4 j1 = make_double4(q2.x, q2.y, q2.z,
+                                      __hiloint2double(0, __float_as_int(q1.w)));
+      const double4 j2 = make_double4(q3.x, q3.y, q3.z, 0.0);
+      pair_dp<ORDER>(I, j0, j1, j2, eps2, S, tmin);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      S.ax += __shfl_xor_sync(0xffffffffu, S.ax, o);
+      S.ay += __shfl_xor_sync(0xffffffffu, S.ay, o);
+      S.az += __shfl_xor_sync(0xffffffffu, S.az, o);
+      S.pot += __shfl_xor_sync(0xffffffffu, S.pot, o);
+      S.jx += __shfl_xor_sync(0xffffffffu, S.jx, o);
+      S.jy += __shfl_xor_sync(0xffffffffu, S.jy, o);
+      S.jz += __shfl_xor_sync(0xffffffffu, S.jz, o);
+      if (ORDER >= SIXTH) {
+        S.sx += __shfl_xor_sync(0xffffffffu, S.sx, o);
+        S.sy += __shfl_xor_sync(0xffffffffu, S.sy, o);
+        S.sz += __shfl_xor_sync(0xffffffffu, S.sz, o);
+      }
+    }
+    if (lane == src) {
+      tot[0 * kBT] += S.ax;
+      tot[1 * kBT] += S.ay;
+      tot[2 * kBT] += S.az;
+      tot[3 * kBT] += S.pot;
+      tot[4 * kBT] += S.jx;
+      tot[5 * kBT] += S.jy;
+      tot[6 * kBT] += S.jz;
+      if (ORDER >= SIXTH) {
+        tot[7 * kBT] += S.sx;
+        tot[8 * kBT] += S.sy;
+        tot[9 * kBT] += S.sz;
+      }
+    }
+  }
+}
+
 template <int RS>
 __device__ __forceinline__ void list_rescan_dp(const IDp &I, bool want, int gi, int row,
                                                int TPI, const double4 *rec, int cnt, int lane,

@@ -5,6 +5,8 @@ C1  4th order, N = 16384 Plummer, all i, lists off (mixed and FP64 kernels)
 C2  6th order, N = 131072, block steps dt = 2^-k, k in 3..12, active sets
     from the block-bin occupancy, lists on (h2 for ~32 neighbours), NN on
 C3  N = 2^20 precision form (Salpeter masses, 10 % binaries), mixed kernel
+    on every i against the FP64 kernel (itself checked against the oracle on
+    a seeded sample), spatial mode on and off
 C4  512 Plummer clusters in one persistent launch (batch API)
 """
 import numpy as np
@@ -68,25 +70,70 @@ def test_c2_sixth_order_131072_block_steps(gpu):
             print(step, len(act), st)
 
 
-def test_c3_precision_form_2_20(gpu):
+@pytest.fixture(scope="module")
+def c3():
+    """The N = 2^20 precision form (seed 3, as the benchmark) and the all-FP64
+    kernel's results on every i (the FP64 kernel is pinned to the oracle in
+    test_c3_fp64_kernel_matches_oracle)."""
     import bench
     cfg = bench.build_inputs(1 << 20, seed=3)
+    cfg["f64"] = _c3_run(cfg, sp.DOUBLE)
+    return cfg
+
+
+def _c3_run(cfg, precision, spatial=None, near=None):
     n = cfg["n"]
-    with sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE, n_pipes=n) as lib:
+    with sp.Sapporo(order=sp.SIXTH, precision=precision, n_pipes=n) as lib:
+        if spatial is not None:
+            lib.set_spatial(spatial, 0.0)
+        if near is not None:
+            lib.set_near(near)
         lib.set_j_particles(np.arange(n), cfg["id"], cfg["t0"], cfg["m"], cfg["x"], cfg["v"],
                             cfg["a"], cfg["j"], cfg["s"], cfg["c"])
         lib.set_time(cfg["ti"])
         lib.start(n, cfg["id"], cfg["px"], cfg["pv"], cfg["pa"], cfg["eps2"], np.zeros(n))
         got = lib.results(n)
+        got["far_tiles"] = lib.spatial_stats()
+    return got
+
+
+def test_c3_fp64_kernel_matches_oracle(gpu, c3):
+    n = c3["n"]
     sel = np.sort(np.random.default_rng(33).choice(n, 512, replace=False)).astype(np.int32)
-    px, pv, pa = O.predict(2, cfg["ti"], cfg["t0"], cfg["x"], cfg["v"], cfg["a"], cfg["j"],
-                           cfg["s"], cfg["c"])
-    want = O.force_subset(2, sel, cfg["px"], cfg["pv"], cfg["pa"], np.zeros(n), cfg["id"], px,
-                          pv, pa, cfg["m"], cfg["id"], cfg["eps2"])
-    sub = {f: got[f][sel] for f in ("acc", "jrk", "snp", "pot")}
-    st = T.check_forces(sub, want, 2)
+    px, pv, pa = O.predict(2, c3["ti"], c3["t0"], c3["x"], c3["v"], c3["a"], c3["j"], c3["s"],
+                           c3["c"])
+    want = O.force_subset(2, sel, c3["px"], c3["pv"], c3["pa"], np.zeros(n), c3["id"], px, pv,
+                          pa, c3["m"], c3["id"], c3["eps2"])
+    sub = {f: c3["f64"][f][sel] for f in ("acc", "jrk", "snp", "pot")}
+    print(T.check_forces(sub, want, 2, 1e-12, 1e-10))
+
+
+@pytest.mark.parametrize("spatial", [1, 0])
+def test_c3_precision_form_2_20_every_i(gpu, c3, spatial):
+    """Mixed precision on all 2^20 i against the FP64 kernel: median <= 1e-6
+    and max <= 1e-4 relative for acc, jerk, snap and pot, in spatial mode (the
+    default for this call size) and in address order."""
+    got = _c3_run(c3, sp.DOUBLESINGLE, spatial=spatial)
+    far, tiles = got["far_tiles"]
+    assert (far > 0.9 * tiles) if spatial else (tiles == 0)
+    st = T.check_forces(got, c3["f64"], 2)
     assert st["acc"][0] <= 1e-6  # the required median relative acc error vs FP64
-    print(st)
+    print(spatial, st)
+
+
+def test_c3_near_pairs_are_summed_in_fp64(gpu, c3):
+    """The FP64 near-pair sums change the results where a j sits within 4
+    softening lengths of an i and nowhere else."""
+    on = _c3_run(c3, sp.DOUBLESINGLE, spatial=0)
+    off = _c3_run(c3, sp.DOUBLESINGLE, spatial=0, near=0.0)
+    changed = np.any(on["snp"] != off["snp"], axis=1)
+    near = (on["ds2min"] < 16 * c3["eps2"]) & (on["ds2min"] > 0)
+    assert changed.sum() > 1000 and np.all(near[changed])
+    e_on = T.rel_err(on["snp"], c3["f64"]["snp"])[changed]
+    e_off = T.rel_err(off["snp"], c3["f64"]["snp"])[changed]
+    print(f"{changed.sum()} i with near pairs: snap max {e_off.max():.2e} -> {e_on.max():.2e}, "
+          f"median {np.median(e_off):.2e} -> {np.median(e_on):.2e}")
+    assert np.median(e_on) < 0.5 * np.median(e_off)
 
 
 def test_c4_ensemble_of_512_clusters(gpu):

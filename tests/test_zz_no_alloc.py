@@ -31,18 +31,25 @@ def _records(case, sel, id_offset=0):
                              case["pa"][sel])
 
 
-def _call(lib, dev, fn, nj, rec, torch, lists=True):
+def _call(lib, dev, fn, nj, rec, torch, lists=True, mem=None):
+    """One force call through the C ABI on device buffers made beforehand;
+    `mem` (a list) receives the device's free bytes just before and after
+    the library call."""
     ni = len(rec)
     i_dev = torch.from_numpy(rec).cuda()
     res = torch.full((ni, sp.RES_STRIDE), np.nan, dtype=torch.float64, device="cuda")
     cnt = torch.full((ni,), -7, dtype=torch.int32, device="cuda")
     lst = torch.full((ni * sp.NGB_PB,), -7, dtype=torch.int32, device="cuda")
     torch.cuda.synchronize()
+    if mem is not None:
+        mem.append(torch.cuda.mem_get_info()[0])
     rc = getattr(lib, fn)(dev, nj, ni, ctypes.c_void_p(i_dev.data_ptr()), 1e-6,
                           sp.F_NGB_LIST if lists else 0, ctypes.c_void_p(res.data_ptr()),
                           ctypes.c_void_p(cnt.data_ptr()), ctypes.c_void_p(lst.data_ptr()))
     assert rc == 0, lib.sapb_last_error(dev).decode()
     torch.cuda.synchronize()
+    if mem is not None:
+        mem.append(torch.cuda.mem_get_info()[0])
     return res.cpu().numpy(), cnt.cpu().numpy(), lst.cpu().numpy().reshape(ni, sp.NGB_PB)
 
 
@@ -64,8 +71,9 @@ def _compare(a, b):
 
 def test_noalloc_matches_device_call_twice(gpu):
     torch = pytest.importorskip("torch")
-    case = T.build_case(2, 3000, seed=61, binaries=0.1)
+    case = T.build_case(2, 16384, seed=61, binaries=0.1)
     n = case["n"]
+    limit = sp.NOALLOC_SCRATCH_BYTES // (8 * sp.RES_STRIDE)
     with sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE) as s:
         s.set_j_particles(np.arange(n), case["id"], case["t0"], case["m"], case["x"], case["v"],
                           case["a"], case["j"], case["s"], case["c"])
@@ -73,16 +81,34 @@ def test_noalloc_matches_device_call_twice(gpu):
         s.force_prediction(n)
         lib, dev = s.lib, s.dev
         s.set_spatial(0)  # both calls in address order: the same arithmetic per pair
-        # first call: every particle
+        # 16 j slices (64 tiles of 256 j): the first call fits them in the
+        # fixed scratch (16384 i x 16 slices), the second (100000 i) does not
+        # and is capped to limit // 100000 = 3 slices
+        s.set_launch(1, 4, 16)
+        assert s.plan(n, n) == (1, 4, 16) and s.plan(100_000, n) == (1, 4, 16)
+        assert 16 * n <= limit and 16 > limit // 100_000
+        # a small call first loads the kernels (module loading may take device
+        # memory); no sapb_force_device call has run yet, so the handle holds
+        # no growable partial-sum buffer: had the next call used one, it
+        # would have had to allocate it and the free memory would show it
+        _call(lib, dev, "sapb_force_device_noalloc", n, _records(case, np.arange(512)), torch)
+        # first compared call: every particle
         rec1 = _records(case, np.arange(n))
-        _compare(_call(lib, dev, "sapb_force_device_noalloc", n, rec1, torch),
-                 _call(lib, dev, "sapb_force_device", n, rec1, torch))
-        # second call in a row on other inputs: a large i set that caps the
-        # j-split to fit the fixed scratch (ids offset: no self pairs)
+        mem = []
+        first = _call(lib, dev, "sapb_force_device_noalloc", n, rec1, torch, mem=mem)
+        assert mem[0] == mem[1], f"free device memory changed by {mem[0] - mem[1]} bytes"
+        _compare(first, _call(lib, dev, "sapb_force_device", n, rec1, torch))
+        # second call in a row on other inputs, over the stale 16-slice
+        # records of the first (ids offset: no self pairs)
         sel = np.random.default_rng(3).integers(0, n, 100_000)
         rec2 = _records(case, sel, id_offset=1_000_000 + np.arange(len(sel)) - case["id"][sel])
         _compare(_call(lib, dev, "sapb_force_device_noalloc", n, rec2, torch),
                  _call(lib, dev, "sapb_force_device", n, rec2, torch))
+        # an empty call does nothing, as sapb_force_device
+        buf = torch.zeros(16, dtype=torch.float64, device="cuda")
+        for fn in ("sapb_force_device_noalloc", "sapb_force_device"):
+            assert getattr(lib, fn)(dev, 0, 0, ctypes.c_void_p(buf.data_ptr()), 0.0, 0,
+                                    ctypes.c_void_p(buf.data_ptr()), None, None) == 0
 
 
 def test_noalloc_rejects_oversize(gpu):
