@@ -38,11 +38,23 @@ FLOPS_4TH, FLOPS_6TH = 38, 60
 METRIC = "interactions/s at N=2^20 mixed vs plain FP64, 1 GPU, acc err<=1e-6; %FP32 peak"
 
 
-# DRAM bytes of one mixed 6th-order force launch at N = 2^20, all i, from
-# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (one pass) of
-# `bench.py --steps 1 --warmup 0 --only mixed --no-cpu` (spatial mode, and with --spatial 0)
-FORCE_DRAM_BYTES = 1060.0e6 + 176.01e6
-FORCE_DRAM_BYTES_ADDRESS_ORDER = 968.47e6 + 182.86e6
+# DRAM bytes (read + written) of one mixed 6th-order force launch at N = 2^20,
+# all i, from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (one
+# pass) of `bench.py --steps 1 --warmup 0 --only mixed` (spatial mode, and
+# with --spatial 0), and the hash of the kernel sources that capture ran
+# (kernel_source_sha).  When the sources change the figure is stale and the
+# bench reports no traffic until it is captured again.
+FORCE_DRAM = {"source_sha": None, "spatial": None, "address": None}
+KERNEL_SOURCES = ["sapb_kernels.cu", "sapb_kernels.cuh", "sapb_pair.cuh", "sapb_internal.cuh",
+                  "sapb_spatial.cu", "sapb_capi.cu"]
+
+
+def kernel_source_sha() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update((ROOT / "sapporo2_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
 
 
 def log(*a):
@@ -135,7 +147,7 @@ LAUNCH_PREC = None  # the precision the override applies to (mixed unless --only
 
 
 def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists=False,
-               shard=None):
+               shard=None, spatial_mode_set=None):
     """Predictor + force on all N with device-resident inputs.  Returns
     per-step predictor / force (+ combine) times (ms) and the results.
 
@@ -143,7 +155,8 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
     rank (the reference's round-robin split over devices) and computes
     their partial forces on every i; the partials are combined by NCCL
     all-reduces (sum of forces, min of nearest-neighbour keys) on the same
-    stream, inside the timed step."""
+    stream, inside the timed step.  spatial_mode_set: spatial mode of the
+    handle (None: the library's default)."""
     import sapporo2_b200 as sp
     from sapporo2_b200.sharded import combine_partials
     n = cfg["n"]
@@ -154,6 +167,8 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
     # a dedicated stream: the library and the timing events must share it
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
+    if spatial_mode_set is not None:
+        s.set_spatial(spatial_mode_set, 0.0)
     if LAUNCH and precision == (LAUNCH_PREC if LAUNCH_PREC is not None else sp.DOUBLESINGLE):
         s.set_launch(*LAUNCH)
     s.set_j_particles(np.arange(nj), cfg["id"][jsel], cfg["t0"][jsel], cfg["m"][jsel],
@@ -196,7 +211,7 @@ def device_arm(cfg, precision: int, steps: int, warmup: int, torch, flush, lists
     out = res.cpu().numpy()
     far_tiles, warp_tiles = s.spatial_stats(reset=True)
     s.close()
-    spatial = precision == sp.DOUBLESINGLE and spatial_on(n, nj)
+    spatial = precision == sp.DOUBLESINGLE and warp_tiles > 0
     # own kernels in the timed steps: predictor, force (+ slice reduction);
     # in spatial mode the j gather, i keys and bounds every step, plus frame
     # init, frame and j keys on the steps that re-sort j (the first call and
@@ -307,12 +322,16 @@ def ensemble_inputs(k: int, seed: int):
     return cl, first, ns
 
 
-def run_ensemble_bench(args, torch):
+def ensemble_leg(torch, steps: int, warmup: int, tune_reps: int = 3) -> dict:
+    """C4: 512 Plummer clusters in one persistent launch per step (batch API,
+    graph replay), after the autotuner.  Device time per step: CUDA events
+    around sapb_batch_run (blob upload + graph replay) on the library's
+    stream; end to end: host wall time of run + results."""
     import sapporo2_b200 as sp
     t_build = time.time()
     cl, first, ns = ensemble_inputs(512, seed=4)
-    log(f"[bench] ensemble of {len(cl)} clusters, {int(ns.sum())} particles built in "
-        f"{time.time() - t_build:.1f}s")
+    build_s = time.time() - t_build
+    log(f"[bench] ensemble of {len(cl)} clusters, {int(ns.sum())} particles built in {build_s:.1f}s")
     total = int(ns.sum())
     act = np.array([len(c["active"]) for c in cl])
     inter = float(np.sum(act * ns))
@@ -333,32 +352,54 @@ def run_ensemble_bench(args, torch):
                 b.i_stage[row:row + len(a)] = sp.pack_i_records(1, c["px"][a], c["pv"][a], None,
                                                                 c["id"][a])
                 row += len(a)
-            tune = b.autotune(sp.F_PREDICT, reps=3)
+            tune = b.autotune(sp.F_PREDICT, reps=tune_reps)
             info = b.info()
-            times = []
-            for it in range(args.warmup + args.steps):
+            wall, dev = [], []
+            for it in range(warmup + steps):
+                e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
                 t0 = time.perf_counter()
+                e0.record(stream)
                 b.run(sp.F_PREDICT)
-                res = b.results()
-                if it >= args.warmup:
-                    times.append(time.perf_counter() - t0)
-    per = float(np.mean(times))
-    dev_ms = tune["ms"]
+                e1.record(stream)
+                b.results()
+                t1 = time.perf_counter()
+                if it >= warmup:
+                    wall.append(t1 - t0)
+                    dev.append(e0.elapsed_time(e1))
+        s.set_stream(None)
+    dev_ms = float(np.mean(dev))
+    per = float(np.mean(wall))
+    return {"value": inter / (dev_ms * 1e-3), "ms_per_step": dev_ms, "steps": steps,
+            "warmup": warmup, "clusters": len(cl), "particles": total,
+            "active_i": int(act.sum()), "interactions_per_step": inter, "autotune": tune,
+            "work_items": info["items"], "persistent_blocks": info["force_blocks"],
+            "e2e": {"value": inter / per, "s_per_step": per,
+                    "h2d_bytes_per_step": int(act.sum()) * 64,
+                    "d2h_bytes_per_step": int(act.sum()) * 96},
+            "inputs_built_s": build_s, "gpu_launches": 3 * steps}
+
+
+def run_ensemble_bench(args, torch):
+    r = ensemble_leg(torch, args.steps, args.warmup)
     print(json.dumps({
         "metric": "interactions/s, ensemble of 512 Plummer clusters (N~logU[256,16384], own t_i, "
                   "active~logU[1/N,1]), Hermite 4th order mixed, one persistent launch per step",
-        "value": inter / (dev_ms * 1e-3), "unit": "interactions/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+        "value": r["value"], "unit": "interactions/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 body",
         "data": "synthetic",
-        "config": {"workload": "ensemble (C4)", "clusters": len(cl), "particles": total,
-                   "active_i": int(act.sum()), "interactions_per_step": inter,
-                   "autotune": tune, "work_items": info["items"],
-                   "persistent_blocks": info["force_blocks"]},
-        "e2e": {"value": inter / per, "unit": "interactions/s", "s_per_step": per,
-                "h2d_bytes_per_step": int(act.sum()) * 64, "d2h_bytes_per_step": int(act.sum()) * 96,
+        "config": {"workload": "ensemble (C4)", "clusters": r["clusters"],
+                   "particles": r["particles"], "active_i": r["active_i"],
+                   "interactions_per_step": r["interactions_per_step"],
+                   "autotune": r["autotune"], "work_items": r["work_items"],
+                   "persistent_blocks": r["persistent_blocks"],
+                   "device_time": "CUDA events around sapb_batch_run (blob upload + graph replay)"},
+        "e2e": {"value": r["e2e"]["value"], "unit": "interactions/s",
+                "s_per_step": r["e2e"]["s_per_step"],
+                "h2d_bytes_per_step": r["e2e"]["h2d_bytes_per_step"],
+                "d2h_bytes_per_step": r["e2e"]["d2h_bytes_per_step"],
                 "api": "sapb_batch_run + sapb_batch_results (tables, i records, graph, results)"},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": r["gpu_launches"],
     }), flush=True)
 
 
@@ -403,6 +444,33 @@ def run_learned_h2_bench(args):
     same = all(np.array_equal(final[k][0], final["fixed"][0]) and
                np.array_equal(final[k][1], final["fixed"][1]) for k in final)
     fr, lr_ = out["fixed"]["retries"], out["learned"]["retries"]
+    # how far the same block steps get with other force arithmetic (the
+    # count-scaled radius; forces do not depend on it): tight binaries make
+    # the time steps sensitive to rounding in the pair sums
+    import sapporo2_b200 as sp
+    variants = {"mixed_address_order": ({"SAPPORO_B200_SPATIAL": "0"}, sp.DOUBLESINGLE),
+                "mixed_address_order_near_off": ({"SAPPORO_B200_SPATIAL": "0",
+                                                  "SAPPORO_B200_NEAR": "0"}, sp.DOUBLESINGLE),
+                "mixed_spatial_near_off": ({"SAPPORO_B200_NEAR": "0"}, sp.DOUBLESINGLE),
+                "fp64": ({}, sp.DOUBLE)}
+    t_end = {"mixed_default": out["count_scaled"]["t_end"]}
+    for name, (env, prec) in variants.items():
+        old_env = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            sim = H.BlockHermite6(cfg["x"], cfg["v"], cfg["m"], cfg["eps2"], H.CountScaledH2(),
+                                  precision=prec)
+            for _ in range(args.c5_steps):
+                sim.step()
+            t_end[name] = float(sim.t.max())
+            sim.close()
+        finally:
+            for k, v in old_env.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        log(f"[bench] learned_h2 t_end {name}: {t_end[name]}")
     print(json.dumps({
         "metric": "neighbour-overflow retries over the block steps, fixed global h2 / learned h2 "
                   "(N=262144 Plummer + 10% binaries, 6th order, target 32, cap 256)",
@@ -411,7 +479,8 @@ def run_learned_h2_bench(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 body, f64 corrector", "data": "synthetic",
         "config": {"workload": "learned h2 (C5)", "n": args.c5_n, "block_steps": args.c5_steps,
-                   "identical_trajectories": bool(same), "policies": out},
+                   "identical_trajectories": bool(same), "policies": out,
+                   "t_end_after_block_steps": t_end},
     }), flush=True)
 
 
@@ -481,15 +550,16 @@ def run_spatial_sizes_bench(args, torch):
     }), flush=True)
 
 
-def run_blocksteps_bench(args):
+def blocksteps_leg(bs_steps: int, modes=("class", "batch")) -> dict:
     """Block time steps of one system (N = 131072 Plummer, 6th order,
     dt = 2^-k with k uniform in 3..12, lists on with h2 for ~32 neighbours):
     the first `bs_steps` block times of the 2^-12 grid, each with the active
     set its block-bin occupancy gives.  Per step the active particles' j
     records are re-staged, then the force on the active set is computed
     (a) through the sapporo class (set_time, startGravCalc, getGravResults)
-    and (b) through the batch API (plan, i records, one graph replay,
-    results).  Host wall time per step, i records prepared beforehand."""
+    and/or (b) through the batch API (plan, i records, one graph replay,
+    results).  Host wall time per step, i records prepared beforehand; every
+    mode runs the steps twice and the second pass is timed."""
     import sapporo2_b200 as sp
     from sapporo2_b200 import ic
     from sapporo2_b200.direct import fp64_direct
@@ -500,7 +570,7 @@ def run_blocksteps_bench(args):
     _, _, sn = fp64_direct(2, x, v, a, m, ids, eps2)
     c = ic.crackle_from(x, a, j)
     steps = []
-    for st in range(1, args.bs_steps + 1):
+    for st in range(1, bs_steps + 1):
         T_, t0, act = ic.block_state(k, st)
         px, pv, pa = ic.predict_fp64(2, T_, t0[act], x[act], v[act], a[act], j[act], sn[act],
                                      c[act])
@@ -509,7 +579,7 @@ def run_blocksteps_bench(args):
     out = {}
     with sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE, n_pipes=n) as s:
         s.set_j_particles(np.arange(n), ids, np.zeros(n), m, x, v, a, j, sn, c)
-        for mode in ("class", "batch", "class", "batch"):  # second pass timed
+        for mode in [md for md in modes for _ in range(2)]:  # second pass timed
             times = []
             b = sp.Batch(s, 1, n) if mode == "batch" else None
             for T_, t0, act, px, pv, pa in steps:
@@ -519,7 +589,7 @@ def run_blocksteps_bench(args):
                 if mode == "class":
                     s.set_time(T_)
                     s.start(n, ids[act], px, pv, pa, eps2, cfg["h2"][act])
-                    r = s.results(n)
+                    s.results(n)
                 else:
                     s.set_no_time()  # the batch run predicts; here only the upload
                     s.force_prediction(n)
@@ -527,7 +597,7 @@ def run_blocksteps_bench(args):
                     b.i_stage[:len(act)] = sp.pack_i_records(2, px, pv, cfg["h2"][act],
                                                              ids[act], pa)
                     b.run(sp.F_PREDICT | sp.F_NGB_LIST)
-                    r = b.results()
+                    b.results()
                 times.append(time.perf_counter() - t_a)
             if b is not None:
                 b.close()
@@ -535,17 +605,56 @@ def run_blocksteps_bench(args):
                          "ms_per_step": 1e3 * float(np.mean(times)),
                          "interactions_per_s": inter / float(np.sum(times))}
     act_n = np.array([len(q[2]) for q in steps])
+    out.update({"n": n, "block_steps": bs_steps, "active_mean": float(act_n.mean()),
+                "active_min": int(act_n.min()), "active_max": int(act_n.max()),
+                "interactions": inter})
+    return out
+
+
+def run_blocksteps_bench(args):
+    r = blocksteps_leg(args.bs_steps)
     print(json.dumps({
         "metric": "interactions/s over block steps (N=131072 Plummer, 6th order, dt=2^-k, "
                   "k in 3..12, lists on), host wall time per step",
-        "value": out["class"]["interactions_per_s"], "unit": "interactions/s", "n_gpus": 1,
-        "steps": args.bs_steps, "warmup": args.bs_steps, "ms_per_step": out["class"]["ms_per_step"],
+        "value": r["class"]["interactions_per_s"], "unit": "interactions/s", "n_gpus": 1,
+        "steps": args.bs_steps, "warmup": args.bs_steps, "ms_per_step": r["class"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 body + ds positions (near tiles) + f64 sums", "data": "synthetic",
-        "config": {"workload": "block steps of one system (C2)", "n": n,
-                   "block_steps": args.bs_steps, "active_mean": float(act_n.mean()),
-                   "active_min": int(act_n.min()), "active_max": int(act_n.max()),
-                   "class_api": out["class"], "batch_api": out["batch"]},
+        "config": {"workload": "block steps of one system (C2)", "n": r["n"],
+                   "block_steps": args.bs_steps, "active_mean": r["active_mean"],
+                   "active_min": r["active_min"], "active_max": r["active_max"],
+                   "class_api": r["class"], "batch_api": r["batch"]},
+    }), flush=True)
+
+
+def run_fma_ceiling_bench(args):
+    """What the FP32 pipe sustains for the force kernel's instruction mixes
+    (bench_fma_ceiling.cu, compiled here for sm_100a): packed FFMA2 chains
+    alone and with one MUFU rsqrt per 16 FFMA2 or one broadcast LDS.128 per
+    32 FFMA2, at 8, 4, 3 and 2 resident 128-thread blocks per SM."""
+    import re
+    import tempfile
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "fma_ceiling")
+        subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                        "-o", exe, str(ROOT / "bench_fma_ceiling.cu")], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    log(out)
+    rows = []
+    for ln in out.splitlines():
+        m = re.match(r"(\d+) blocks/SM\s+(\S+)\s+([\d.]+) ms\s+([\d.]+) TFLOP/s\s+([\d.]+) %", ln)
+        if m:
+            rows.append({"blocks_per_sm": int(m.group(1)), "mix": m.group(2),
+                         "tflops": float(m.group(4)), "frac_nominal": float(m.group(5)) / 100})
+    ceil = {(r["blocks_per_sm"], r["mix"]): r["frac_nominal"] for r in rows}
+    print(json.dumps({
+        "metric": "FP32-pipe ceiling: fraction of nominal FP32 peak sustained by FFMA2 chains "
+                  "with one MUFU per 16 FFMA2, 2 resident blocks/SM",
+        "value": ceil.get((2, "ffma2+mufu")), "unit": "fraction of nominal", "n_gpus": 1,
+        "steps": 3, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "fma_ceiling probe (bench_fma_ceiling.cu)", "rows": rows},
     }), flush=True)
 
 
@@ -618,18 +727,23 @@ def main():
     ap.add_argument("--impl", default="sapporo_b200")
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--fp64-steps", type=int, default=2)
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--address-steps", type=int, default=2,
+                    help="timed steps of the address-order (spatial mode off) arm")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the block-step (C2) and ensemble (C4) legs of the default run")
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2", "blocksteps",
-                                           "spatial_sizes"],
+                                           "spatial_sizes", "fma_ceiling"],
                     default="precision",
                     help="precision: the N=2^20 6th-order bench line; ensemble: 512 clusters; "
                          "learned_h2: block steps with fixed, count-scaled and learned h2; "
                          "blocksteps: block steps of one system, class vs batch API; "
                          "spatial_sizes: predict + force per call, address order vs spatial "
-                         "mode, over call sizes")
+                         "mode, over call sizes; fma_ceiling: what the FP32 pipe sustains for "
+                         "the force kernel's instruction mixes")
     ap.add_argument("--bs-steps", type=int, default=64)
     ap.add_argument("--multi", choices=["shard", "replicas"], default="shard",
                     help="N>1 GPUs: shard: one N-body system, j split over the ranks "
@@ -653,6 +767,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "fma_ceiling":
+        run_fma_ceiling_bench(args)
         return
     if args.launch:
         global LAUNCH, LAUNCH_PREC
@@ -734,12 +851,47 @@ def main():
         f64_ms = np.array([float(t.item())])
     f64_value = inter_step / (f64_ms.mean() * 1e-3)  # per job
 
+    # the same mixed kernels in address order (double-single difference on
+    # every pair, the reference's arithmetic), beside the spatial-mode line
+    addr = None
+    if mix["spatial"]:
+        addr = device_arm(cfg, sp.DOUBLESINGLE, args.address_steps, 1, torch, flush, shard=shard,
+                          spatial_mode_set=0)
+        a_ms = np.array(addr["pred_ms"]) + np.array(addr["force_ms"]) + np.array(addr["comb_ms"])
+        if dist:
+            t = torch.tensor([float(a_ms.mean())], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            a_ms = np.array([float(t.item())])
+        addr["value"] = inter_step * jobs / (a_ms.mean() * 1e-3)
+        addr["ms_per_step"] = float(a_ms.mean())
+
     e2e = e2e_arm(cfg, args.e2e_steps, shard=shard)
     e2e_value = inter_step / e2e["s_per_step"]
     if dist:
         t = torch.tensor([e2e["s_per_step"]], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_value = inter_step * jobs / float(t.item())
+
+    # short legs on one GPU: block steps of one system through the class (C2)
+    # and the 512-cluster ensemble in one persistent launch (C4)
+    legs = {}
+    if world == 1 and not args.no_legs:
+        bl = blocksteps_leg(16, modes=("class",))
+        legs["blocksteps_c2"] = {
+            "value": bl["class"]["interactions_per_s"], "unit": "interactions/s",
+            "ms_per_step": bl["class"]["ms_per_step"], "block_steps": bl["block_steps"],
+            "active_mean": bl["active_mean"], "active_min": bl["active_min"],
+            "active_max": bl["active_max"], "n": bl["n"],
+            "timing": "host wall time per block step through the sapporo class (j re-staged, "
+                      "set_time, startGravCalc, getGravResults), second of two passes"}
+        en = ensemble_leg(torch, steps=5, warmup=2, tune_reps=1)
+        legs["ensemble_c4"] = {
+            "value": en["value"], "unit": "interactions/s", "ms_per_step": en["ms_per_step"],
+            "steps": en["steps"], "clusters": en["clusters"], "particles": en["particles"],
+            "active_i": en["active_i"], "interactions_per_step": en["interactions_per_step"],
+            "autotune": en["autotune"], "e2e": en["e2e"],
+            "timing": "CUDA events around sapb_batch_run (blob upload + graph replay), after "
+                      "the autotuner"}
 
     if rank != 0:
         if dist:
@@ -761,6 +913,15 @@ def main():
     pred_bytes = 224.0  # FP64 inputs 19 doubles read + 9 values written, per j
     pred_read_write = (19 * 8 + 64)  # bytes actually moved by this predictor (64-B record out)
     pred_ms = float(np.mean(mix["pred_ms"]))
+
+    sha = kernel_source_sha()
+    traffic, traffic_note = None, (
+        f"no ncu capture of this kernel source (sha {sha}); the last capture was of "
+        f"{FORCE_DRAM['source_sha']}")
+    if FORCE_DRAM["source_sha"] == sha and n == 1 << 20 and nj_loc == n:
+        traffic = FORCE_DRAM["spatial" if mix["spatial"] else "address"]
+        traffic_note = ("dram__bytes_read.sum + dram__bytes_write.sum of one force_kernel<6th,DS> "
+                        f"launch at N=2^20 (ncu, 1 pass) of this kernel source (sha {sha})")
 
     result = {
         "metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": world,
@@ -791,14 +952,8 @@ def main():
                  "speedup_mixed_over_fp64": value / jobs / f64_value},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak,
-                     "traffic": ((FORCE_DRAM_BYTES if mix["spatial"] else
-                                  FORCE_DRAM_BYTES_ADDRESS_ORDER)
-                                 if (n == 1 << 20 and nj_loc == n) else None),
-                     "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                     "force_kernel<6th,DS> launch at N=2^20 (ncu, 1 pass): "
-                                     "1060 MB read + 176 MB written in 1.86 s, 0.66 GB/s (spatial mode; "
-                                     "address order 968 + 183 MB in 2.03 s); "
-                                     "j records stream from L2",
+                     "traffic": traffic,
+                     "traffic_note": traffic_note,
                      "peak_note": f"derived: {nsm} SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz "
                                   "(sm_max_mhz of measured peaks; no FP32 entry there)",
                      "frac_at_run_clock": achieved / fp32_peak_run,
@@ -818,10 +973,21 @@ def main():
         "gpu_launches": mix["launches"],
     }
     # accuracy: mixed vs all-FP64 GPU kernel on all N
+    fields = (("acc", slice(0, 3)), ("pot", slice(3, 4)), ("jrk", slice(4, 7)),
+              ("snp", slice(7, 10)))
     rm, rd = mix["res"], f64["res"]
-    result["accuracy_vs_fp64_gpu"] = {k: rel_stats(rm[:, sl], rd[:, sl]) for k, sl in
-                                      (("acc", slice(0, 3)), ("jrk", slice(4, 7)),
-                                       ("snp", slice(7, 10)))}
+    result["accuracy_vs_fp64_gpu"] = {k: rel_stats(rm[:, sl], rd[:, sl]) for k, sl in fields}
+    if addr is not None:
+        result["address_order"] = {
+            "value": addr["value"], "unit": "interactions/s", "ms_per_step": addr["ms_per_step"],
+            "force_ms": float(np.mean(addr["force_ms"])), "steps": args.address_steps,
+            "frac_fp32_peak": FLOPS_6TH * float(n) * nj_loc
+                              / (float(np.mean(addr["force_ms"])) * 1e-3) / 1e12 / fp32_peak,
+            "note": "the same mixed kernels with the spatial mode off: double-single position "
+                    "difference on every pair (the reference's arithmetic)",
+            "accuracy_vs_fp64_gpu": {k: rel_stats(addr["res"][:, sl], rd[:, sl])
+                                     for k, sl in fields}}
+    result.update(legs)
     if not args.no_cpu and world == 1:
         cb = cpu_baseline_leg(cfg, args.cpu_sample)
         o, sel = cb["oracle"], cb["sel"]
@@ -830,8 +996,8 @@ def main():
             "sample": f"{len(sel)} seeded i x all {n} j, FP64 OpenMP, {cb['seconds']:.1f} s"}
         acc_m = {}
         for name, res in (("mixed", rm), ("fp64_gpu", rd)):
-            acc_m[name] = {k: rel_stats(res[sel][:, s3], o[k]) for k, s3 in
-                           (("acc", slice(0, 3)), ("jrk", slice(4, 7)), ("snp", slice(7, 10)))}
+            acc_m[name] = {k: rel_stats(res[sel][:, s3], o[k] if k != "pot" else o[k][:, None])
+                           for k, s3 in fields}
         result["accuracy_vs_fp64_oracle"] = acc_m
     print(json.dumps(result), flush=True)
     if dist:

@@ -1,13 +1,14 @@
-// fma_ceiling -- what the FP32 pipe of this GPU sustains for instruction
-// mixes like the force kernel's, so the force kernel's fraction of the
-// nominal FP32 peak can be read against a measured ceiling.
+// fma_ceiling -- a measurement probe, not part of the library: what the FP32
+// pipe of this GPU sustains for instruction mixes like the force kernel's, so
+// the force kernel's fraction of the nominal FP32 peak can be read against a
+// measured ceiling.  Compiled and run by
 //
-//   sapporo2_b200/lib/fma_ceiling
+//   python bench.py --workload fma_ceiling
 //
 // Each test runs independent chains of FP32 FMAs (scalar FFMA or packed
 // FP32x2 __ffma2_rn) for a fixed count and reports FMA lane-operations/s as
-// TFLOP/s (2 flops per FMA), at 8 and at 2 resident 128-thread blocks per SM
-// (the force kernel runs 2).  Mixes:
+// TFLOP/s (2 flops per FMA), at 8, 4, 3 and 2 resident 128-thread blocks per
+// SM (the force kernel runs 2 or 3).  Mixes:
 //   ffma        scalar FFMA, 16 chains
 //   ffma2       packed FFMA2, 8 float2 chains
 //   ffma2+mufu  one rsqrt.approx (MUFU) per 16 FFMA2 (+2 FADD feeding it)
@@ -116,7 +117,7 @@ int main() {
   float *out = nullptr;
   if (cudaMalloc(&out, sizeof(float) * nsm * 8 * kThreads) != cudaSuccess) return 1;
   const char *names[4] = {"ffma", "ffma2", "ffma2+mufu", "ffma2+lds"};
-  for (int bps : {8, 2}) {
+  for (int bps : {8, 4, 3, 2}) {
     const int blocks = nsm * bps;
     // FMA lane-operations per thread: 128 per iteration in every mode
     const double ops = (double)blocks * kThreads * iters * 128.0;

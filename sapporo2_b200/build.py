@@ -109,9 +109,6 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     if rely or not liby.exists():
         _run([HOST_CXX, "-shared", "-o", str(liby), str(objy), f"-L{LIBDIR}", "-lsapporo_b200",
               "-Wl,-rpath,$ORIGIN", "-Wl,-Bsymbolic"])
-    src_c, bin_c = CSRC / "fma_ceiling.cu", LIBDIR / "fma_ceiling"
-    if force or _stale(bin_c, src_c, []):
-        _run([NVCC, *ARCH, "-O3", "-std=c++17", "-ccbin", HOST_CXX, "-o", str(bin_c), str(src_c)])
     if verbose:
         print(f"built {lib}")
     return lib

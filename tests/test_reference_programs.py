@@ -19,19 +19,30 @@ import pytest
 import sapporo2_b200 as sp
 
 ROOT = Path(__file__).resolve().parents[1]
-REF = Path(os.environ.get("SAPPORO_REFERENCE", "/root/reference"))
 REF_BIN = ROOT / "oracle" / "_ref"
+
+
+def _reference_tree() -> Path | None:
+    """The reference tree: SAPPORO_REFERENCE, else the one oracle/Makefile
+    built oracle/_ref/ from (recorded in oracle/_ref/reference_path)."""
+    env = os.environ.get("SAPPORO_REFERENCE")
+    if env:
+        return Path(env)
+    rec = REF_BIN / "reference_path"
+    return Path(rec.read_text().strip()) if rec.exists() else None
+
 PROGRAMS = ["test_integrator", "test_gravity_block", "test_gravity_block_6th"]
 
 
 @pytest.mark.parametrize("prog", PROGRAMS)
 def test_reference_program_links_unchanged(prog, tmp_path):
-    src = REF / "testCodes" / "src" / f"{prog}.cpp"
-    if not src.exists():
+    ref = _reference_tree()
+    src = ref / "testCodes" / "src" / f"{prog}.cpp" if ref else None
+    if src is None or not src.exists():
         pytest.skip("reference tree not present")
     lib = sp.LIB_PATH
     cmd = ["/usr/bin/g++", "-O1", "-w", "-fopenmp", f"-I{ROOT / 'include'}",
-           f"-I{REF / 'testCodes' / 'src'}", str(src), "-o", str(tmp_path / prog),
+           f"-I{ref / 'testCodes' / 'src'}", str(src), "-o", str(tmp_path / prog),
            f"-L{lib.parent}", "-lsapporo_b200", f"-Wl,-rpath,{lib.parent}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
