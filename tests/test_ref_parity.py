@@ -94,3 +94,102 @@ def test_small_steps_match_reference(gpu, ni):
     _snap_vs_oracle(case, got, sel=sel)
     T.check_nn(case, got["nnb"], ref, sel=sel)
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], ref, sel=sel)
+
+
+# ---- the workloads at their own sizes (reference geometry: 256-i launches) ----
+def _c1_case():
+    from sapporo2_b200 import ic
+    cfg = ic.make_config("C1")
+    n = cfg["n"]
+    a, j, _ = O.derivative_fn()(1, cfg["x"], cfg["v"], None, cfg["m"], cfg["id"], cfg["eps2"])
+    rpx, rpv, _ = O.ref_predict(1, cfg["ti"], cfg["t0"], cfg["x"], cfg["m"], cfg["v"], a, j)
+    return dict(order=1, n=n, x=cfg["x"], v=cfg["v"], m=cfg["m"], a=a, j=j, s=None, c=None,
+                id=cfg["id"], t0=cfg["t0"], ti=cfg["ti"], px=rpx, pv=rpv, pa=None,
+                h2=np.zeros(n), eps2=cfg["eps2"])
+
+
+@pytest.mark.parametrize("precision", [sp.DOUBLESINGLE, sp.DOUBLE])
+def test_c1_16384_all_i_matches_reference(gpu, precision):
+    """C1 (4th order, N = 16384 Plummer, all i, lists off) against the
+    reference's fourth_DS / fourth_double (kernels.cu:1100-1102)."""
+    _ref_ready()
+    case = _c1_case()
+    n = case["n"]
+    assert O.ref_size_ok(1, n)  # no padded i-threads in the reference launch
+    ref = O.ref_gravity(1, precision, case["px"], case["pv"], None, case["h2"], case["id"],
+                        case["px"], case["pv"], None, case["m"], case["id"], case["eps2"])
+    got = T.run_library(case, precision, lists=False)
+    stats = T.check_forces(got, ref, 1, fields=REF_FIELDS)
+    ties = T.check_nn(case, got["nnb"], ref)
+    assert ties <= 2 and n == 16384
+    print(f"C1 prec {precision}: {stats} nn-ties {ties}")
+
+
+_C2 = {}
+
+
+def _c2_case(step):
+    """C2 (6th order, N = 131072 Plummer, block steps dt = 2^-k, k in 3..12,
+    h2 for ~32 neighbours) at block time step * 2^-12: j predicted by the
+    reference's own predictor, the active set from the block-bin occupancy."""
+    from sapporo2_b200 import ic
+    from sapporo2_b200.direct import fp64_direct
+    if "base" not in _C2:
+        cfg = ic.make_config("C2")
+        x, v, m, ids, eps2 = cfg["x"], cfg["v"], cfg["m"], cfg["id"], cfg["eps2"]
+        a, j, _ = fp64_direct(1, x, v, None, m, ids, eps2)
+        _, _, s = fp64_direct(2, x, v, a, m, ids, eps2)
+        _C2["base"] = (cfg, a, j, s, ic.crackle_from(x, a, j))
+    cfg, a, j, s, c = _C2["base"]
+    T_, t0, act = ic.block_state(cfg["k"], step)
+    rpx, rpv, rpa = O.ref_predict(2, T_, t0, cfg["x"], cfg["m"], cfg["v"], a, j, s, c)
+    case = dict(order=2, n=cfg["n"], x=cfg["x"], v=cfg["v"], m=cfg["m"], a=a, j=j, s=s, c=c,
+                id=cfg["id"], t0=t0, ti=T_, px=rpx, pv=rpv, pa=rpa, h2=cfg["h2"],
+                eps2=cfg["eps2"])
+    return case, act
+
+
+def _c2_ref(case, sel, precision):
+    ref = O.ref_gravity(2, precision, case["px"][sel], case["pv"][sel], case["pa"][sel],
+                        case["h2"][sel], case["id"][sel], case["px"], case["pv"], case["pa"],
+                        case["m"], case["id"], case["eps2"])
+    ref["ngb_list"] = np.sort(np.where(np.arange(256)[None, :] < ref["ngb_count"][:, None],
+                                       ref["ngb_list"], np.iinfo(np.int32).max), axis=1)
+    return ref
+
+
+@pytest.mark.parametrize("precision", [sp.DOUBLESINGLE, sp.DOUBLE])
+def test_c2_block_step_matches_reference(gpu, precision):
+    """C2's first block step (the 12983 particles with dt = 2^-12) on all
+    131072 j, lists and nearest neighbours on, against the reference's
+    sixth_DS / sixth_double (kernels.cu:1104-1106); snap against the oracle."""
+    _ref_ready()
+    case, act = _c2_case(1)
+    assert len(act) >= 12983
+    ref = _c2_ref(case, act, precision)
+    got = T.run_library(case, precision, sel=act)
+    stats = T.check_forces(got, ref, 2, fields=REF_FIELDS)
+    _snap_vs_oracle(case, got, sel=act)
+    ties = T.check_nn(case, got["nnb"], ref, sel=act)
+    exempt = T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], ref, sel=act)
+    assert ties <= 2 and np.median(ref["ngb_count"]) > 10
+    print(f"C2 step 1 prec {precision}: {len(act)} i {stats} nn-ties {ties} boundary {exempt}")
+
+
+def test_spatial_call_matches_reference(gpu):
+    """One call above the spatial-mode threshold (4096 i x 131072 j = 2^29
+    pairs: Morton order, single-float difference on far tiles) against the
+    reference's sixth_DS, lists and nearest neighbours on."""
+    _ref_ready()
+    case, _ = _c2_case(1)
+    sel = np.sort(np.random.default_rng(71).choice(case["n"], 4096, replace=False))
+    ref = _c2_ref(case, sel, sp.DOUBLESINGLE)
+    got = T.run_library(case, sp.DOUBLESINGLE, sel=sel, spatial=(1, 0.0))
+    far, tiles = got["far_tiles"]
+    assert far > 0.5 * tiles > 0  # the call really ran in spatial mode
+    stats = T.check_forces(got, ref, 2, fields=REF_FIELDS)
+    _snap_vs_oracle(case, got, sel=sel)
+    ties = T.check_nn(case, got["nnb"], ref, sel=sel)
+    exempt = T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], ref, sel=sel)
+    assert ties <= 2
+    print(f"spatial call: far {far}/{tiles} {stats} nn-ties {ties} boundary {exempt}")
