@@ -269,6 +269,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
   // the single-float difference, are within 2 sqrt(3) delta (relative) of the
   // exact ones on a far tile.
   const float shrink = spatial ? fminf(0.9999f, 1.f - 8.f * (0x1p-23f / A.far_c)) : 1.f;
+  const float shrink_e = shrink * (1.f - 8.f * 0x1p-24f);
   bool broken = false;
   int nfar = 0;  // far tiles of this warp (spatial mode)
 
@@ -434,9 +435,14 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
             best[p] = tmin[p];
             best_tile[p] = it;
           }
+          // far tiles: tmin is the smallest single-float ds2 + eps2 (softening
+          // folded in, each of its 3 roundings within 2^-24), so a pair
+          // below h2 gives tmin * shrink (1 - 8 2^-24) < h2 + eps2
           if (A.do_list)
-            list_rescan_mix<C::RS>(Im[p], (far ? tmin[p] * shrink : tmin[p]) < Im[p].h2, oi[p],
-                                   ty, TPI, rec, cnt, lane, A.ngb_count, A.ngb_list);
+            list_rescan_mix<C::RS>(Im[p],
+                                   far ? (valid[p] && tmin[p] * shrink_e < Im[p].h2 + eps2f)
+                                       : (tmin[p] < Im[p].h2),
+                                   oi[p], ty, TPI, rec, cnt, lane, A.ngb_count, A.ngb_list);
         }
       }
     }

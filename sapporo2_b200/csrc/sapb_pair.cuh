@@ -285,11 +285,13 @@ __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, cons
 // Far tile (spatial mode): the j tile and the warp's i are at least
 // |x|max * 2^-23 / delta apart, so the difference of the high parts alone,
 // xj_hi - xi_hi, is within delta (relative) of the double-single one (each
-// low part is below 2^-24 |x|): 3 FMA-pipe operations instead of 9.  No pair
-// of such a tile can be a nearest neighbour (the caller checks that against
-// the i's bounds); with LIST the minimum of this approximate ds2 is kept so
-// the caller can rescan the tile exactly for list members.  The self pair is
-// still masked by id.
+// low part is below 2^-24 |x|): 3 FMA-pipe operations instead of 9, and the
+// softening enters the first FMA of the squared distance (one operation
+// less; no pair of a far tile is a nearest neighbour, so its unsoftened ds2
+// is not needed: the caller checks that against the i's bounds).  With LIST
+// the minimum of this approximate softened ds2 is kept so the caller can
+// rescan the tile exactly for list members.  The self pair is still masked
+// by id.
 template <int ORDER, bool LIST>
 __device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, const float4 &r1,
                                               const float4 &r2, const float4 &r3, float2 eps2,
@@ -303,12 +305,11 @@ __device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, 
     P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
     P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
   }
-  const float2 ds2 = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dx, P.dx)));
+  const float2 r2v = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __ffma2_rn(P.dx, P.dx, eps2)));
   if (LIST) {
-    tmin.x = fminf(tmin.x, ds2.x);
-    tmin.y = fminf(tmin.y, ds2.y);
+    tmin.x = fminf(tmin.x, r2v.x);
+    tmin.y = fminf(tmin.y, r2v.y);
   }
-  const float2 r2v = __fadd2_rn(ds2, eps2);
   P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
   pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
