@@ -429,6 +429,7 @@ def run_learned_h2_bench(args):
             "overflow_rate": st["overflow"] / ev, "overflows": st["overflow"],
             "retries": st["retries"], "retry_rounds": st["rounds"],
             "in_range_frac": st["in_range"] / ev, "evaluations": st["evaluated"],
+            "in_25pct_frac": st["in_tight"] / ev, "mean_abs_log_count_err": st["abs_log_err"] / ev,
             "ms_per_step": 1e3 * st["step_s"] / max(st["steps"], 1),
             "force_ms_per_step": 1e3 * st["force_s"] / max(st["steps"], 1),
             "train_ms_per_step": 1e3 * getattr(sim.policy, "train_s", 0.0) / max(st["steps"], 1),

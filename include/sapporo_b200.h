@@ -218,12 +218,14 @@ int sapb_mlp_forward(sapb_mlp *m, int n, const float *x, float *y);
 int sapb_mlp_gradient(sapb_mlp *m, int n, const float *x, const float *t, float *grad,
                       float *loss);
 /* `epochs` full-batch Adam steps (lr, beta 0.9/0.999); loss before the last. */
-/* Radius proposal in one call: in = n records of 8 floats (previous
- * neighbour count, previous h2, acceleration[3], jerk[3]); the features
- * (logarithms of the density estimate n/(4/3 pi h^3), |a|, |jerk|, 1 + n, h2,
- * n = max(count, 1/2)) are standardised with mu[5], sd[5]; the network's
- * correction, clipped to [-max_down, max_up], is added to the count-scaled
- * step 2/3 log(target/n); h2_out = h2 * exp(step clipped to +-clip). */
+/* Radius proposal in one call: in = n records of 9 floats (previous
+ * neighbour count, previous h2, acceleration[3], jerk[3], L = the particle's
+ * running mean of log density over its past evaluations); the features
+ * (log rho with the density estimate rho = n/(4/3 pi h^3), n = max(count,
+ * 1/2), log |a|, log |jerk|, L - log rho, log h2) are standardised with mu[5],
+ * sd[5]; the network's correction, clipped to [-max_down, max_up], is added
+ * to the count-scaled step 2/3 log(target/n); h2_out = h2 * exp(step clipped
+ * to +-clip). */
 int sapb_mlp_propose(sapb_mlp *m, int n, const float *in, const float *mu, const float *sd,
                      float target, float max_down, float max_up, float clip, float *h2_out);
 int sapb_mlp_train(sapb_mlp *m, int n, const float *x, const float *t, int epochs, float lr,
@@ -271,7 +273,8 @@ int sapb_spatial_stats(sapb_dev *d, unsigned long long *far_tiles,
  * it off (every pair in FP32, as the reference); the default is 16 (pairs
  * within 4 softening lengths).  The environment variable SAPPORO_B200_NEAR
  * sets the factor at open.  No effect with eps2 = 0 or on the FP64 and
- * GRAPE-5 kernels.  Batch calls take every pair in FP32. */
+ * GRAPE-5 kernels.  Batch calls take the factor in force when they are
+ * planned (sapb_batch_plan). */
 int sapb_set_near(sapb_dev *d, double factor);
 
 #ifdef __cplusplus

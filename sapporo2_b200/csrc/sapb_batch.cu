@@ -179,8 +179,11 @@ int sapb_batch_plan(sapb_batch *b, int n_clusters, const int *j_first, const int
       return sapb_fail(d, SAPB_EINVAL, "cluster %d has active i but no j", c);
     prev_end = j_first[c] + j_count[c];
     j_extent = std::max(j_extent, prev_end);
+    const double e2 = eps2 ? eps2[c] : 0.0;
+    const float nr2 = (d->prec == SAPB_DOUBLE || d->order == SAPB_GRAPE5)
+                          ? 0.0f : (float)(d->near_k * e2);
     cl[c] = BatchCluster{j_first[c], j_count[c], i_first, i_count[c], 1, 0,
-                         t_pred ? t_pred[c] : 0.0, eps2 ? eps2[c] : 0.0};
+                         t_pred ? t_pred[c] : 0.0, e2, nr2, 0};
     i_first += i_count[c];
     if (i_count[c] > 0) {
       tpi[c] = tpi_rule(i_count[c], b->tpi_scale);

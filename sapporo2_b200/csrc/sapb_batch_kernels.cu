@@ -209,11 +209,22 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
             {Q.ax.x, Q.ay.x, Q.az.x, -Q.pot.x, Q.jx.x, Q.jy.x, Q.jz.x, Q.sx.x, Q.sy.x, Q.sz.x},
             {Q.ax.y, Q.ay.y, Q.az.y, -Q.pot.y, Q.jx.y, Q.jy.y, Q.jz.y, Q.sx.y, Q.sy.y, Q.sz.y}};
         const float tmin[2] = {tm.x, tm.y};
+        const float near_r2 = B.cl[W.cluster].near_r2;
 #pragma unroll
         for (int p = 0; p < 2; p++) {
           double *t = tot + (size_t)p * 10 * kBT + tid;
+          // a near pair in this row: the row is summed again in FP64
+          // (near_rescan_mix) and its FP32 partial is dropped
+          const bool nearp = ORDER != GRAPE5 && valid[p] && tmin[p] < near_r2;
+          if (!nearp) {
 #pragma unroll
-          for (int f = 0; f < 10; f++) t[f * kBT] += (double)qv[p][f];
+            for (int f = 0; f < 10; f++) t[f * kBT] += (double)qv[p][f];
+          }
+          if (ORDER != GRAPE5) {
+            const unsigned nm = __ballot_sync(0xffffffffu, nearp);
+            if (nm) near_rescan_mix<ORDER, C::RS>(nm, gi[p], ty, tpi, rec, cnt, lane, B.irec,
+                                                  eps2d, t);
+          }
           if (tmin[p] < best[p]) {
             best[p] = tmin[p];
             best_tile[p] = it;

@@ -96,6 +96,8 @@ struct BatchCluster {
   int nslices;           // j-split of this cluster (1: items write results directly)
   int part_base;         // first partial record of this cluster
   double t_pred, eps2;
+  float near_r2;         // mixed precision: near pairs (ds2 < near_r2) summed in FP64; 0 off
+  int pad_;
 };
 struct BatchItem {
   int cluster;

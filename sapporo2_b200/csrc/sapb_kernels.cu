@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
         if (ORDER != GRAPE5) {
           const unsigned nm = __ballot_sync(0xffffffffu, nearp);
           if (nm)
-            near_rescan_mix<ORDER, C::RS, TPI>(nm, oi[p], ty, rec, cnt, lane, A.irec, A.eps2, t);
+            near_rescan_mix<ORDER, C::RS>(nm, oi[p], ty, TPI, rec, cnt, lane, A.irec, A.eps2, t);
         }
         if (ORDER != GRAPE5) {  // GRAPE-5: no nearest neighbour, no lists
           // a far tile holds no nearest neighbour; its minimum is the

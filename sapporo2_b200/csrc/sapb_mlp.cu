@@ -77,16 +77,17 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(const float *__restric
 }
 
 // Proposal: the five features of each particle from its raw previous state
-// (n_prev, h2_prev, a[3], jerk[3]; logarithms of the density estimate
-// n / (4/3 pi h^3), |a|, |jerk|, 1 + n, h2 with n = max(n_prev, 1/2)),
-// standardised with (mu, sd), the network's correction clipped to
-// [-max_down, max_up] and added to the count-scaled step 2/3 log(target/n);
-// out: h2_prev * exp(clip(step, -clip, clip)).
+// (n_prev, h2_prev, a[3], jerk[3], L; features: log rho with the density
+// estimate rho = n / (4/3 pi h^3), n = max(n_prev, 1/2), log |a|, log |jerk|,
+// L - log rho with L the particle's running mean of log rho over its past
+// evaluations, log h2), standardised with (mu, sd), the network's correction
+// clipped to [-max_down, max_up] and added to the count-scaled step
+// 2/3 log(target/n); out: h2_prev * exp(clip(step, -clip, clip)).
 struct MlpScale {
   float mu[kIn], sd[kIn];
   float target, max_down, max_up, clip;
 };
-constexpr int kPropIn = 8;
+constexpr int kPropIn = 9;
 
 __global__ void __launch_bounds__(128) mlp_propose_kernel(const float *__restrict__ P, int n,
                                                           const float *__restrict__ IN,
@@ -101,8 +102,8 @@ __global__ void __launch_bounds__(128) mlp_propose_kernel(const float *__restric
   const float an = sqrtf(r[2] * r[2] + r[3] * r[3] + r[4] * r[4]) + 1e-30f;
   const float jn = sqrtf(r[5] * r[5] + r[6] * r[6] + r[7] * r[7]) + 1e-30f;
   const float lh2 = logf(h2);
-  const float f[kIn] = {logf(np) - logf(4.18879020f) - 1.5f * lh2, logf(an), logf(jn),
-                        log1pf(np), lh2};
+  const float lrho = logf(np) - logf(4.18879020f) - 1.5f * lh2;
+  const float f[kIn] = {lrho, logf(an), logf(jn), r[8] - lrho, lh2};
   float x[kIn];
 #pragma unroll
   for (int k = 0; k < kIn; k++) x[k] = (f[k] - sc.mu[k]) / sc.sd[k];

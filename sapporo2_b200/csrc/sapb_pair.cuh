@@ -421,10 +421,10 @@ __device__ __forceinline__ void list_rescan_mix(const IMix &I, bool want, int gi
 // double; velocity, acceleration and mass as stored) against the i's own FP64
 // record, and the warp sum is added to that i's FP64 totals by its lane.
 // `nm` is the ballot of the lanes that asked; rare, so kept out of line.
-template <int ORDER, int RS, int TPI>
-__device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, const float4 *rec,
-                                             int cnt, int lane, const double *irec, double eps2,
-                                             double *tot) {
+template <int ORDER, int RS>
+__device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, int tpi,
+                                             const float4 *rec, int cnt, int lane,
+                                             const double *irec, double eps2, double *tot) {
   while (nm) {
     const int src = __ffs(nm) - 1;
     nm &= nm - 1;
@@ -441,7 +441,7 @@ __device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, const
     }
     AccDp S{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     double tmin = DBL_MAX;
-    for (int k = srow + lane * TPI; k < cnt; k += 32 * TPI) {
+    for (int k = srow + lane * tpi; k < cnt; k += 32 * tpi) {
       const float4 q0 = rec[k * RS + 0], q1 = rec[k * RS + 1], q2 = rec[k * RS + 2];
       const float4 q3 = ORDER >= SIXTH ? rec[k * RS + 3] : q2;
       const double4 j0 = make_double4((double)q0.x + (double)q1.x, (double)q0.y + (double)q1.y,

@@ -18,7 +18,7 @@ import time
 import numpy as np
 
 from . import DOUBLESINGLE, NGB_PB, SIXTH, Sapporo
-from .learned_h2 import TARGET, H2Net, features, retry_h2, target_log_ratio
+from .learned_h2 import TARGET, H2Net, features, log_density, retry_h2, target_log_ratio
 
 # [C, P, Q] = M^-1 [A, J, S] for the quintic interpolation of a(t)
 _MINV = np.linalg.inv(np.array([[1 / 6, 1 / 24, 1 / 120], [1 / 2, 1 / 6, 1 / 24],
@@ -61,15 +61,20 @@ class CountScaledH2:
 
 class LearnedH2:
     """The GPU-trained network proposes h2 from the particle's previous
-    evaluation (as a correction to the count-scaled radius).  It is
-    pretrained on the counts of the two start-up force passes (two radii)
-    and then learns online from first-attempt counts."""
+    evaluation and its history (as a correction to the count-scaled radius).
+    It is pretrained on the counts of the two start-up force passes (two
+    radii) and then learns online from first-attempt counts.  The history is
+    a running mean of each particle's log density over its evaluations
+    (weight `w` on the newest), kept here and updated after every step."""
 
     name = "learned"
 
     def __init__(self, sap, seed=5, epochs=4, lr=1e-3, pre_epochs=300, max_batch=8192,
-                 max_pre=65536, train_every=4):
+                 max_pre=65536, train_every=4, w=0.5):
         self.net = H2Net(sap, seed=seed)
+        # start from a zero correction: the count-scaled radius is already a
+        # good proposal, the network only adds what it learns consistently
+        self.net.zero_output_layer()
         self.epochs, self.lr, self.pre_epochs = epochs, lr, pre_epochs
         self.max_batch, self.max_pre, self.train_every = max_batch, max_pre, train_every
         self.rng = np.random.default_rng(seed)
@@ -78,9 +83,12 @@ class LearnedH2:
         self.pretrain_s = 0.0
         self.propose_s = 0.0
         self.n_obs = 0
+        self.w = w
+        self.lrho = None  # running mean of log density per particle
 
     def start(self, sim, samples):
         t0 = time.perf_counter()
+        self.lrho = log_density(sim.n_prev, sim.h2_prev)
         f = np.concatenate([s[0] for s in samples])
         y = np.concatenate([s[1] - self.net.base_log_ratio(s[2]) for s in samples])
         if len(f) > self.max_pre:
@@ -93,25 +101,28 @@ class LearnedH2:
 
     def propose(self, sim, idx):
         t0 = time.perf_counter()
-        h2 = self.net.propose(sim.n_prev[idx], sim.h2_prev[idx], sim.a[idx], sim.j[idx])
+        h2 = self.net.propose(sim.n_prev[idx], sim.h2_prev[idx], sim.a[idx], sim.j[idx],
+                              self.lrho[idx])
         self.propose_s += time.perf_counter() - t0
         return h2
 
     def observe(self, sim, idx, h2_used, counts):
         """One online update on (at most max_batch of) this step's first
-        attempts, every train_every-th block step."""
+        attempts, every train_every-th block step; then the history of the
+        evaluated particles takes in this step's counts."""
         self.n_obs += 1
-        if (self.n_obs - 1) % self.train_every:
-            return
-        t0 = time.perf_counter()
-        take = np.arange(len(idx))
-        if len(take) > self.max_batch:
-            take = self.rng.choice(len(idx), self.max_batch, replace=False)
-        q = idx[take]
-        loss = self.net.learn(sim.n_prev[q], sim.h2_prev[q], sim.a[q], sim.j[q], h2_used[take],
-                              counts[take], epochs=self.epochs, lr=self.lr)
-        self.losses.append(loss)
-        self.train_s += time.perf_counter() - t0
+        if (self.n_obs - 1) % self.train_every == 0:
+            t0 = time.perf_counter()
+            take = np.arange(len(idx))
+            if len(take) > self.max_batch:
+                take = self.rng.choice(len(idx), self.max_batch, replace=False)
+            q = idx[take]
+            loss = self.net.learn(sim.n_prev[q], sim.h2_prev[q], sim.a[q], sim.j[q],
+                                  h2_used[take], counts[take], lrho_mean=self.lrho[q],
+                                  epochs=self.epochs, lr=self.lr)
+            self.losses.append(loss)
+            self.train_s += time.perf_counter() - t0
+        self.lrho[idx] += self.w * (log_density(counts, h2_used) - self.lrho[idx])
 
 
 def half_mass_h2(x, m, target=TARGET):
@@ -143,8 +154,8 @@ class BlockHermite6:
         self.t = np.zeros(self.n)
         self.h2_fix = half_mass_h2(self.x, self.m)
         self.stats = {"evaluated": 0, "overflow": 0, "retries": 0, "rounds": 0,
-                      "in_range": 0, "force_s": 0.0, "step_s": 0.0, "steps": 0,
-                      "interactions": 0.0}
+                      "in_range": 0, "in_tight": 0, "abs_log_err": 0.0, "force_s": 0.0,
+                      "step_s": 0.0, "steps": 0, "interactions": 0.0}
         # two passes at t = 0: acc and jerk, then snap with the i acceleration;
         # their neighbour counts (radii h2_fix / 4 and h2_fix) are the
         # policies' start-up samples
@@ -203,6 +214,9 @@ class BlockHermite6:
             over = over[c2 >= NGB_PB]
         self.stats["evaluated"] += len(idx)
         self.stats["in_range"] += int(np.sum((first >= TARGET / 2) & (first <= 2 * TARGET)))
+        # a tighter band (+-25 % in the count) and the mean |log(count/target)|
+        self.stats["in_tight"] += int(np.sum((first >= 0.75 * TARGET) & (first <= 1.25 * TARGET)))
+        self.stats["abs_log_err"] += float(np.sum(np.abs(np.log(np.maximum(first, 0.5) / TARGET))))
         self.stats["force_s"] += time.perf_counter() - t0
         self.h2_used, self.first_counts = h2, first
         return r, cnt

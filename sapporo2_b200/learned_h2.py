@@ -2,12 +2,15 @@
 particle's h2 from five features of its previous force evaluation, and is
 trained online on the neighbour counts the force kernel reports.
 
-Features (all logarithmic, standardised with statistics frozen at the first
-training call): local density estimate n_prev / (4/3 pi h_prev^3), |a|,
-|jerk|, 1 + n_prev, h2_prev.  The proposal is
+Features (standardised with statistics frozen at the first training call):
+log of the local density estimate rho = n_prev / (4/3 pi h_prev^3), log |a|,
+log |jerk|, the particle's running mean L of log rho over its past
+evaluations less log rho (how far the last count strays from the
+particle's history: Poisson noise of a count of ~32 is ~18 %), log h2_prev.
+The proposal is
 log(h2 / h2_prev) = 2/3 log(target / n_prev) + network output: the network
 learns the correction to the count-scaled radius (density drift along the
-orbit, regression of noisy small counts).  Target for a particle evaluated
+orbit, shrinkage of a noisy last count toward the particle's history).  Target for a particle evaluated
 with h2_used that found n neighbours: the radius that would have given the
 target count in a locally uniform medium,
 log(h2_used / h2_prev) + 2/3 log(target / max(n, 1/2)), minus the
@@ -29,13 +32,22 @@ TARGET = 32.0
 CAP = 256
 
 
-def features(n_prev, h2_prev, acc, jrk) -> np.ndarray:
-    n = np.maximum(np.asarray(n_prev, dtype=np.float64), 0.5)
+def log_density(n, h2) -> np.ndarray:
+    """log of n / (4/3 pi h^3), n = max(count, 1/2)."""
+    n = np.maximum(np.asarray(n, dtype=np.float64), 0.5)
+    return np.log(n / (4.0 / 3.0 * np.pi * np.asarray(h2, dtype=np.float64) ** 1.5))
+
+
+def features(n_prev, h2_prev, acc, jrk, lrho_mean=None) -> np.ndarray:
+    """The network's five inputs (before standardisation); lrho_mean is the
+    particle's running mean of log density (None: no history yet, the last
+    evaluation's own value)."""
     h2 = np.asarray(h2_prev, dtype=np.float64)
-    rho = n / (4.0 / 3.0 * np.pi * h2 ** 1.5)
+    lr = log_density(n_prev, h2)
+    lm = lr if lrho_mean is None else np.asarray(lrho_mean, dtype=np.float64)
     a = np.linalg.norm(acc, axis=1) + 1e-30
     j = np.linalg.norm(jrk, axis=1) + 1e-30
-    return np.stack([np.log(rho), np.log(a), np.log(j), np.log1p(n), np.log(h2)], axis=1)
+    return np.stack([lr, np.log(a), np.log(j), lm - lr, np.log(h2)], axis=1)
 
 
 def target_log_ratio(h2_used, h2_prev, n_obs, target=TARGET) -> np.ndarray:
@@ -72,6 +84,14 @@ class H2Net:
         _check(self.lib.sapb_mlp_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))),
                "mlp_get", self.owner.dev)
         return p
+
+    def zero_output_layer(self):
+        """Output weights and bias set to zero (the last 65 parameters, W4
+        and b4): the network then proposes no correction until training
+        finds a consistent one."""
+        p = self.params()
+        p[-(64 + 1):] = 0.0
+        self.set_params(p)
 
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
@@ -134,19 +154,20 @@ class H2Net:
     MAX_DOWN = 1.0
     MAX_UP = 0.25
 
-    def propose(self, n_prev, h2_prev, acc, jrk, clip=4.0) -> np.ndarray:
+    def propose(self, n_prev, h2_prev, acc, jrk, lrho_mean=None, clip=4.0) -> np.ndarray:
         """h2 for the next evaluation: the count-scaled radius times the
         network's bounded correction; the whole log-ratio is clipped to
         +-clip.  Features, standardisation, network and correction run in
         one kernel (sapb_mlp_propose) from the raw per-particle state."""
         if self.mu is None:
-            self.fit_standardisation(features(n_prev, h2_prev, acc, jrk))
+            self.fit_standardisation(features(n_prev, h2_prev, acc, jrk, lrho_mean))
         n = len(h2_prev)
-        rec = np.empty((n, 8), dtype=np.float32)
+        rec = np.empty((n, 9), dtype=np.float32)
         rec[:, 0] = n_prev
         rec[:, 1] = h2_prev
         rec[:, 2:5] = acc
         rec[:, 5:8] = jrk
+        rec[:, 8] = log_density(n_prev, h2_prev) if lrho_mean is None else lrho_mean
         mu = self._f(self.mu)
         sd = self._f(self.sd)
         out = np.empty(n, dtype=np.float32)
@@ -157,19 +178,20 @@ class H2Net:
                                          out.ctypes.data_as(fp)), "mlp_propose", self.owner.dev)
         return out.astype(np.float64)
 
-    def propose_host(self, n_prev, h2_prev, acc, jrk, clip=4.0) -> np.ndarray:
+    def propose_host(self, n_prev, h2_prev, acc, jrk, lrho_mean=None, clip=4.0) -> np.ndarray:
         """The same proposal with the features built on the host (FP64) and
         only the network on the GPU -- the reference for propose()."""
-        f = self.standardise(features(n_prev, h2_prev, acc, jrk))
+        f = self.standardise(features(n_prev, h2_prev, acc, jrk, lrho_mean))
         corr = np.clip(self.forward(f).astype(np.float64), -self.MAX_DOWN, self.MAX_UP)
         r = self.base_log_ratio(n_prev) + corr
         return np.asarray(h2_prev) * np.exp(np.clip(r, -clip, clip))
 
-    def learn(self, n_prev, h2_prev, acc, jrk, h2_used, n_obs, epochs=20, lr=2e-3) -> float:
+    def learn(self, n_prev, h2_prev, acc, jrk, h2_used, n_obs, lrho_mean=None, epochs=20,
+              lr=2e-3) -> float:
         """One online update: the correction that would have given the target
         count, from the count the force kernel found with h2_used (clipped to
         the correction's bounds, so a particle that found no neighbour does
         not drag the fit)."""
-        f = self.standardise(features(n_prev, h2_prev, acc, jrk))
+        f = self.standardise(features(n_prev, h2_prev, acc, jrk, lrho_mean))
         y = target_log_ratio(h2_used, h2_prev, n_obs) - self.base_log_ratio(n_prev)
         return self.train(f, np.clip(y, -self.MAX_DOWN, self.MAX_UP), epochs, lr)

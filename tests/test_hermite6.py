@@ -58,17 +58,25 @@ def test_integrator_conserves_energy_and_radius_does_not_change_forces():
 
 @pytest.mark.gpu
 def test_learned_radius_cuts_overflow_retries(gpu):
+    """Against the fixed global radius the learned one cuts overflow retries
+    >= 5x; against the count-scaled radius (no network) it takes no more
+    retries and lands as many lists in [16, 64] within 1 %."""
     x, v, m, eps2 = _cluster(32768, seed=5)
     runs = {}
-    for name in ("fixed", "learned"):
-        pol = H.FixedH2() if name == "fixed" else (lambda sap: H.LearnedH2(sap, seed=5))
-        sim = H.BlockHermite6(x, v, m, eps2, pol)
+    policies = {"fixed": H.FixedH2, "count_scaled": H.CountScaledH2,
+                "learned": lambda: (lambda sap: H.LearnedH2(sap, seed=5))}
+    for name, make in policies.items():
+        sim = H.BlockHermite6(x, v, m, eps2, make())
         for _ in range(40):
             sim.step()
         runs[name] = (sim.x.copy(), sim.v.copy(), dict(sim.stats))
         sim.close()
-    (xf, vf, sf), (xl, vl, sl) = runs["fixed"], runs["learned"]
+    (xf, vf, sf), (xc, vc, sc), (xl, vl, sl) = runs["fixed"], runs["count_scaled"], runs["learned"]
     # equal step results: forces do not depend on the radius
     assert np.array_equal(xf, xl) and np.array_equal(vf, vl)
+    assert np.array_equal(xc, xl) and np.array_equal(vc, vl)
     assert sf["retries"] >= 5 * max(sl["retries"], 1), (sf, sl)
     assert sl["in_range"] > sf["in_range"], (sf, sl)
+    assert sl["retries"] <= sc["retries"], (sc, sl)
+    assert sl["in_range"] >= 0.99 * sc["in_range"], (sc, sl)
+    print({k: (r[2]["retries"], r[2]["in_range"] / r[2]["evaluated"]) for k, r in runs.items()})

@@ -85,9 +85,12 @@ def test_gpu_proposal_kernel_matches_the_host_features(gpu):
     h2 = 10.0 ** rng.uniform(-6, -1, n)
     acc = rng.normal(size=(n, 3)) * 10.0 ** rng.uniform(-2, 2, (n, 1))
     jrk = rng.normal(size=(n, 3)) * 10.0 ** rng.uniform(-1, 3, (n, 1))
+    from sapporo2_b200.learned_h2 import log_density
+    hist = log_density(n_prev, h2) + rng.normal(scale=0.3, size=n)
     with sp.Sapporo(order=sp.SIXTH) as s:
         net = H2Net(s, seed=13)
-        want = net.propose_host(n_prev, h2, acc, jrk)
-        got = net.propose(n_prev, h2, acc, jrk)
+        for lm in (None, hist):
+            want = net.propose_host(n_prev, h2, acc, jrk, lm)
+            got = net.propose(n_prev, h2, acc, jrk, lm)
+            np.testing.assert_allclose(got, want, rtol=2e-5)
         net.close()
-    np.testing.assert_allclose(got, want, rtol=2e-5)
