@@ -44,7 +44,8 @@ METRIC = "interactions/s at N=2^20 mixed vs plain FP64, 1 GPU, acc err<=1e-6; %F
 # with --spatial 0), and the hash of the kernel sources that capture ran
 # (kernel_source_sha).  When the sources change the figure is stale and the
 # bench reports no traffic until it is captured again.
-FORCE_DRAM = {"source_sha": None, "spatial": None, "address": None}
+FORCE_DRAM = {"source_sha": "c5c8a1cbf6e3d611",
+              "spatial": 1103934720.0 + 110644736.0, "address": 1059357696.0 + 190586368.0}
 KERNEL_SOURCES = ["sapb_kernels.cu", "sapb_kernels.cuh", "sapb_pair.cuh", "sapb_internal.cuh",
                   "sapb_spatial.cu", "sapb_capi.cu"]
 
@@ -403,15 +404,13 @@ def run_ensemble_bench(args, torch):
     }), flush=True)
 
 
-def run_learned_h2_bench(args):
-    """The learned-h2 workload: N=262144 Plummer + 10 % binaries, 6th-order
-    block steps, neighbour lists on (target 32, cap 256), the same steps run
-    with the fixed global radius, the count-scaled radius and the learned
-    radius.  Forces do not depend on the radius (in spatial mode too: its
-    far test ignores h2), so the three trajectories are identical; the
-    policies differ in overflows, retries and time."""
+def learned_h2_leg(n: int, steps: int):
+    """C5: N Plummer + 10 % binaries, 6th-order block steps, neighbour lists
+    on (target 32, cap 256), the same steps run with the fixed global
+    radius, the count-scaled radius and the learned radius.  Returns the
+    per-policy statistics and the final states."""
     from sapporo2_b200 import hermite6 as H, ic
-    cfg = ic.make_config("C5", n=args.c5_n, seed=5)
+    cfg = ic.make_config("C5", n=n, seed=5)
     policies = {"fixed": lambda: H.FixedH2(), "count_scaled": lambda: H.CountScaledH2(),
                 "learned": lambda: (lambda sap: H.LearnedH2(sap, seed=5))}
     out, final = {}, {}
@@ -420,7 +419,7 @@ def run_learned_h2_bench(args):
         sim = H.BlockHermite6(cfg["x"], cfg["v"], cfg["m"], cfg["eps2"], make())
         t_init = time.perf_counter() - t0
         active = []
-        for _ in range(args.c5_steps):
+        for _ in range(steps):
             active.append(sim.step())
         de = abs(sim.energy() - sim.e0) / abs(sim.e0)
         st = dict(sim.stats)
@@ -444,6 +443,17 @@ def run_learned_h2_bench(args):
         sim.close()
     same = all(np.array_equal(final[k][0], final["fixed"][0]) and
                np.array_equal(final[k][1], final["fixed"][1]) for k in final)
+    return cfg, out, same
+
+
+def run_learned_h2_bench(args):
+    """The learned-h2 workload (learned_h2_leg at N = 262144, 200 block
+    steps) plus how far the same steps get with other force arithmetic.
+    Forces do not depend on the radius (in spatial mode too: its far test
+    ignores h2), so the policies' trajectories are identical; the policies
+    differ in overflows, retries and time."""
+    from sapporo2_b200 import hermite6 as H
+    cfg, out, same = learned_h2_leg(args.c5_n, args.c5_steps)
     fr, lr_ = out["fixed"]["retries"], out["learned"]["retries"]
     # how far the same block steps get with other force arithmetic (the
     # count-scaled radius; forces do not depend on it): tight binaries make
@@ -733,7 +743,8 @@ def main():
                     help="timed steps of the address-order (spatial mode off) arm")
     ap.add_argument("--no-legs", action="store_true",
                     help="skip the block-step (C2) and ensemble (C4) legs of the default run")
-    ap.add_argument("--cpu-sample", type=int, default=2048)
+    ap.add_argument("--cpu-sample", type=int, default=16384,
+                    help="i of the timed CPU-baseline sample (x all N j; about 10 s on 16 host threads)")
     ap.add_argument("--ref-sample", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["precision", "ensemble", "learned_h2", "blocksteps",
@@ -885,6 +896,14 @@ def main():
             "active_max": bl["active_max"], "n": bl["n"],
             "timing": "host wall time per block step through the sapporo class (j re-staged, "
                       "set_time, startGravCalc, getGravResults), second of two passes"}
+        _, lh, same = learned_h2_leg(262144, 200)
+        legs["learned_h2_c5"] = {
+            "value": lh["fixed"]["retries"] / max(lh["learned"]["retries"], 1),
+            "unit": "x fewer overflow retries (fixed global h2 / learned h2)",
+            "n": 262144, "block_steps": 200, "identical_trajectories": bool(same),
+            "policies": {k: {q: v[q] for q in ("retries", "in_range_frac", "in_25pct_frac",
+                                                "mean_abs_log_count_err", "ms_per_step",
+                                                "t_end")} for k, v in lh.items()}}
         en = ensemble_leg(torch, steps=5, warmup=2, tune_reps=1)
         legs["ensemble_c4"] = {
             "value": en["value"], "unit": "interactions/s", "ms_per_step": en["ms_per_step"],

@@ -48,7 +48,8 @@ __global__ void __launch_bounds__(256) batch_predict_kernel(BatchArgs B) {
 // ring keeps a block-wide tile counter across items, so its mbarrier phases
 // continue from item to item without re-initialisation.
 template <int ORDER, int PREC>
-__global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_kernel(BatchArgs B) {
+__global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3 : 4)))
+    batch_force_kernel(BatchArgs B) {
   using C = FCfg<ORDER, PREC, 2, 2>;  // shared-memory plan with a row reduction area
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : 4)) batch_force_ker
           }
           if (ORDER != GRAPE5) {
             const unsigned nm = __ballot_sync(0xffffffffu, nearp);
-            if (nm) near_rescan_mix<ORDER, C::RS>(nm, gi[p], ty, tpi, rec, cnt, lane, B.irec,
+            if (nm) near_rescan_inl<ORDER, C::RS>(nm, gi[p], ty, tpi, rec, cnt, lane, B.irec,
                                                   eps2d, t);
           }
           if (tmin[p] < best[p]) {

@@ -2,6 +2,8 @@
 // See sapb_kernels.cuh for the list and sapb_internal.cuh for the layouts.
 #include <float.h>
 
+#include <algorithm>
+
 #include "sapb_kernels.cuh"
 #include "sapb_launch.h"
 #include "sapb_pair.cuh"
@@ -52,14 +54,16 @@ __global__ void __launch_bounds__(256) scatter_kernel(const double *__restrict__
 // Reads the FP64 structure-of-arrays state with one coalesced 8-byte load
 // per component and writes the force record of each j.
 // ========================================================================
+// The grid is one wave of resident blocks striding over the j (a grid of
+// nj / 256 blocks would leave its last wave part-empty: 2^20 j are 3.5 waves).
 template <int ORDER, int PREC>
 __global__ void __launch_bounds__(256) predict_kernel(int nj, double ti, JState js, void *pred) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nj) return;
-  double p[3], v[3], a[3];
-  taylor<ORDER>(js, k, ti, p, v, a);
-  store_record<ORDER, PREC>(pred, k, p[0], p[1], p[2], __ldg(js.m + k), __ldg(js.id + k), v[0],
-                            v[1], v[2], a[0], a[1], a[2]);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nj; k += gridDim.x * blockDim.x) {
+    double p[3], v[3], a[3];
+    taylor<ORDER>(js, k, ti, p, v, a);
+    store_record<ORDER, PREC>(pred, k, p[0], p[1], p[2], __ldg(js.m + k), __ldg(js.id + k),
+                              v[0], v[1], v[2], a[0], a[1], a[2]);
+  }
 }
 
 // Readback of j[first, first+n): raw FP64 state and its FP64 prediction to
@@ -424,8 +428,16 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
         }
         if (ORDER != GRAPE5) {
           const unsigned nm = __ballot_sync(0xffffffffu, nearp);
-          if (nm)
-            near_rescan_mix<ORDER, C::RS>(nm, oi[p], ty, TPI, rec, cnt, lane, A.irec, A.eps2, t);
+          if (nm) {
+            // out of line where the register budget has room for the call,
+            // inlined where the shape is held to 128 or 168 registers
+            if constexpr (C::MIN_BLOCKS >= 3)
+              near_rescan_inl<ORDER, C::RS>(nm, oi[p], ty, TPI, rec, cnt, lane, A.irec, A.eps2,
+                                            t);
+            else
+              near_rescan_mix<ORDER, C::RS>(nm, oi[p], ty, TPI, rec, cnt, lane, A.irec, A.eps2,
+                                            t);
+          }
         }
         if (ORDER != GRAPE5) {  // GRAPE-5: no nearest neighbour, no lists
           // a far tile holds no nearest neighbour; its minimum is the
@@ -625,7 +637,18 @@ template <int ORDER, int PREC>
 static cudaError_t launch_predict_t(int nj, double ti, const JState &js, void *pred,
                                     cudaStream_t st) {
   if (nj <= 0) return cudaSuccess;
-  predict_kernel<ORDER, PREC><<<(nj + 255) / 256, 256, 0, st>>>(nj, ti, js, pred);
+  static int wave = 0;  // resident blocks on the whole device (one per instantiation)
+  if (!wave) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, predict_kernel<ORDER, PREC>, 256, 0);
+    if (e != cudaSuccess) return e;
+    wave = std::max(1, sms * occ);
+  }
+  const int blocks = std::min((nj + 255) / 256, wave);
+  predict_kernel<ORDER, PREC><<<blocks, 256, 0, st>>>(nj, ti, js, pred);
   return cudaGetLastError();
 }
 

@@ -85,7 +85,10 @@ struct FCfg {
   // resident blocks per SM the register budget is held to: FP64 kernels sit
   // at 168 registers, where one more allocation step (176) drops them from
   // 3 to 2 blocks per SM and costs 7 % at N = 2^20 (6th order)
-  static constexpr int MIN_BLOCKS = PREC == DOUBLE ? 3 : (IP >= 4 ? 2 : 4);
+  // (mixed 6th order with 2 i per thread: 3, since at 128 registers the FP64
+  // near-pair rescan spills)
+  static constexpr int MIN_BLOCKS =
+      PREC == DOUBLE ? 3 : (IP >= 4 ? 2 : (ORDER >= SIXTH && IP == 2 ? 3 : 4));
 };
 
 // ---------------- mixed precision pair ----------------
@@ -420,11 +423,14 @@ __device__ __forceinline__ void list_rescan_mix(const IMix &I, bool want, int gi
 // record widened to double (the double-single position hi + lo is exact in
 // double; velocity, acceleration and mass as stored) against the i's own FP64
 // record, and the warp sum is added to that i's FP64 totals by its lane.
-// `nm` is the ballot of the lanes that asked; rare, so kept out of line.
+// `nm` is the ballot of the lanes that asked.  near_rescan_mix keeps it out
+// of line (the grid kernel, whose register budget has room for the call);
+// near_rescan_inl is the same code inlined (the batch kernel, held to 128
+// registers, where the call would spill).
 template <int ORDER, int RS>
-__device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, int tpi,
-                                             const float4 *rec, int cnt, int lane,
-                                             const double *irec, double eps2, double *tot) {
+__device__ __forceinline__ void near_rescan_inl(unsigned nm, int oi, int row, int tpi,
+                                                const float4 *rec, int cnt, int lane,
+                                                const double *irec, double eps2, double *tot) {
   while (nm) {
     const int src = __ffs(nm) - 1;
     nm &= nm - 1;
@@ -481,6 +487,13 @@ __device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, int t
       }
     }
   }
+}
+
+template <int ORDER, int RS>
+__device__ __noinline__ void near_rescan_mix(unsigned nm, int oi, int row, int tpi,
+                                             const float4 *rec, int cnt, int lane,
+                                             const double *irec, double eps2, double *tot) {
+  near_rescan_inl<ORDER, RS>(nm, oi, row, tpi, rec, cnt, lane, irec, eps2, tot);
 }
 
 template <int RS>

@@ -69,7 +69,7 @@ class LearnedH2:
 
     name = "learned"
 
-    def __init__(self, sap, seed=5, epochs=4, lr=1e-3, pre_epochs=300, max_batch=8192,
+    def __init__(self, sap, seed=5, epochs=1, lr=1e-4, pre_epochs=300, max_batch=8192,
                  max_pre=65536, train_every=4, w=0.5):
         self.net = H2Net(sap, seed=seed)
         # start from a zero correction: the count-scaled radius is already a

@@ -33,9 +33,11 @@ def make_ensemble(order, k, seed, nmin=64, nmax=1500):
     return clusters
 
 
-def run_ensemble(order, precision, clusters, lists=True, tuning=0, reps=1):
+def run_ensemble(order, precision, clusters, lists=True, tuning=0, reps=1, near=None):
     total = sum(c["n"] for c in clusters)
     with sp.Sapporo(order=order, precision=precision) as s:
+        if near is not None:
+            s.set_near(near)
         addr = 0
         j_first, j_count, i_count, t_pred, eps2 = [], [], [], [], []
         for c in clusters:
@@ -93,6 +95,35 @@ def test_ensemble_matches_oracle(gpu, order, precision):
         k = len(c["active"])
         check_cluster(order, precision, c, res[row:row + k], cnt[row:row + k], lst[row:row + k])
         row += k
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_ensemble_near_pairs_in_fp64(gpu, order):
+    """The batch kernel sums the rows of tiles holding a near pair (ds2 < 16
+    eps2) in FP64: results change exactly for the i with such a pair, and
+    the changed ones move closer to the oracle."""
+    clusters = make_ensemble(order, 12, seed=31 + order)
+    for c in clusters:  # a softening of 1e-2: pairs within 4e-2 are near ones
+        c["eps2"] = 1e-4
+    on = run_ensemble(order, sp.DOUBLESINGLE, clusters, lists=False)[0]
+    off = run_ensemble(order, sp.DOUBLESINGLE, clusters, lists=False, near=0.0)[0]
+    row, e_on, e_off, n_changed = 0, [], [], 0
+    for c in clusters:
+        a = c["active"]
+        k = len(a)
+        ro, rf = on[row:row + k], off[row:row + k]
+        changed = np.any(ro[:, 0:10] != rf[:, 0:10], axis=1)
+        near = (ro[:, 10] < 16 * c["eps2"]) & (ro[:, 11] >= 0)
+        assert np.array_equal(changed, near), c["n"]
+        want = T.oracle_force(c, sel=a, lists=False)
+        f, sl = ("snp", slice(7, 10)) if order >= 2 else ("jrk", slice(4, 7))
+        for r, e in ((ro, e_on), (rf, e_off)):
+            e.append(T.rel_err(r[:, sl], want[f])[changed])
+        n_changed += int(changed.sum())
+        row += k
+    e_on, e_off = np.concatenate(e_on), np.concatenate(e_off)
+    assert n_changed > 30, n_changed
+    assert np.median(e_on) < np.median(e_off), (np.median(e_on), np.median(e_off))
 
 
 @pytest.mark.parametrize("tuning", [-2, 1, 3])
