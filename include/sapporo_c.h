@@ -20,6 +20,10 @@ sapporo_c *sapporo_c_new(void);
 void sapporo_c_delete(sapporo_c *s);
 /* sapporo::open with a one-device list {device}. */
 int sapporo_c_open(sapporo_c *s, int device, int order, int precision);
+/* sapporo::open(kernelFile, devices, ndev, order, precision): ndev > 0 uses
+ * devices[0..ndev-1] (ids may repeat), 0 every visible device, < 0 the
+ * first -ndev devices.  j are spread round-robin over them by address. */
+int sapporo_c_open_devices(sapporo_c *s, int ndev, const int *devices, int order, int precision);
 int sapporo_c_close(sapporo_c *s);
 int sapporo_c_get_n_pipes(sapporo_c *s);
 int sapporo_c_set_time(sapporo_c *s, double ti);
@@ -45,7 +49,11 @@ int sapporo_c_retrieve_predicted(sapporo_c *s, int addr, double *out);
 /* out: mass, id, eps2, pos[3], vel[3], acc[3], jrk[3], ppos[3], pvel[3], pacc[3] (24). */
 int sapporo_c_retrieve_state(sapporo_c *s, int addr, double *out);
 int sapporo_c_last_status(sapporo_c *s);
+/* The device handle of the first device (sapporo_c_device) and of entry k
+ * of the device list (null when k is out of range); their number. */
 struct sapb_dev *sapporo_c_device(sapporo_c *s);
+struct sapb_dev *sapporo_c_device_at(sapporo_c *s, int k);
+int sapporo_c_n_devices(sapporo_c *s);
 
 #ifdef __cplusplus
 }

@@ -5,8 +5,8 @@
  * (lib/include/sapporohostclass.h:37-176): same class name, method names,
  * argument order and meaning, default arguments and enum values, so callers
  * written against the reference compile and link unchanged.  The private
- * part is this library's own (one GPU behind the sapb_* C ABI of
- * sapporo_b200.h); no binary layout compatibility is implied.
+ * part is this library's own (one sapb_* device handle of sapporo_b200.h per
+ * device given to open); no binary layout compatibility is implied.
  *
  * Like the reference header it pulls in <iostream>, <vector>, <map>,
  * <string>, <cmath> and `using namespace std`, which its callers rely on.
@@ -46,7 +46,11 @@ struct sapb_dev;
 
 class sapporo {
  protected:
-  sapb_dev *dev_;
+  // One handle per device of open(); j address a lives on devs_[a % G] at
+  // local address a / G (G = devs_.size()), as the reference distributes j
+  // round-robin over its devices (lib/src/sapporohostclass.cpp:473-474).
+  std::vector<sapb_dev *> devs_;
+  sapb_dev *dev_;       // devs_[0]
   int n_pipes;
   int nj_max;           // allocated j capacity (addresses below it are accepted)
   int integrationOrder;
@@ -57,10 +61,10 @@ class sapporo {
   bool nj_updated;      // j staged since the last push
   bool predJOnHost;     // host cache of the predicted j state is current
 
-  // j staging: slot of each address staged since the last push, -1 if none
+  // j staging: slot of each address staged since the last push (in the
+  // staging of its device), -1 if none; per device the staged addresses
   std::vector<int> stage_slot_;
-  std::vector<int> staged_addr_;
-  int nstaged_;
+  std::vector<std::vector<int> > staged_addr_;
 
   // per-address prediction time of the force records (NaN: unpredicted copy)
   std::vector<double> pred_time_;
@@ -69,10 +73,14 @@ class sapporo {
 
   int dev_ni;                    // i count of the last force call
   int nj_last_;
-  std::vector<int> ngb_count_h_;
-  std::vector<int> ngb_list_h_;
+  std::vector<int> dev_nj_;      // per device: j of the last force call
+  std::vector<std::vector<int> > ngb_count_h_;  // per device
+  std::vector<std::vector<int> > ngb_list_h_;
   bool ngb_fetched_;
 
+  int ndev() const { return (int)devs_.size(); }
+  int nj_on(int g, int nj) const;  // j among the first nj addresses held by device g
+  double *stage_record(int address, int &rc);
   int push_staged();
   void increase_jMemory();
   int refresh_jcache(int addr);
@@ -118,11 +126,13 @@ class sapporo {
   int get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, int nbl[]);
 
   // Additions of this library (not in the reference): the underlying device
-  // handle, the status of the last call that can fail (0 = ok), and n calls
+  // handles, the status of the last call that can fail (0 = ok), and n calls
   // of set_j_particle in one (arrays of n, vectors [n][3]; a, jrk, snp, crk,
   // eps, t may be null for zeros): the same address rules, one staging
-  // reservation for all.
+  // reservation per device for all.
   sapb_dev *device_handle() { return dev_; }
+  sapb_dev *device_handle(int k) { return k >= 0 && k < ndev() ? devs_[k] : nullptr; }
+  int n_devices() const { return ndev(); }
   int last_status;
   int set_j_particles(int n, const int *address, const int *id, const double *t,
                       const double *mass, const double *x, const double *v, const double *a,

@@ -127,6 +127,7 @@ _SIGS = [
     ("sapporo_c_new", C.c_void_p, []),
     ("sapporo_c_delete", None, [C.c_void_p]),
     ("sapporo_c_open", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    ("sapporo_c_open_devices", C.c_int, [C.c_void_p, C.c_int, _ipo, C.c_int, C.c_int]),
     ("sapporo_c_close", C.c_int, [C.c_void_p]),
     ("sapporo_c_get_n_pipes", C.c_int, [C.c_void_p]),
     ("sapporo_c_set_time", C.c_int, [C.c_void_p, C.c_double]),
@@ -144,6 +145,8 @@ _SIGS = [
     ("sapporo_c_retrieve_state", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("sapporo_c_last_status", C.c_int, [C.c_void_p]),
     ("sapporo_c_device", C.c_void_p, [C.c_void_p]),
+    ("sapporo_c_device_at", C.c_void_p, [C.c_void_p, C.c_int]),
+    ("sapporo_c_n_devices", C.c_int, [C.c_void_p]),
     # GRAPE-6
     # GRAPE-5 interface
     ("g5_open_special", C.c_int, [C.c_int, C.POINTER(C.c_int)]),
@@ -241,11 +244,14 @@ def _i32(a):
 
 
 class Sapporo:
-    """The ``sapporo`` class (C++), one GPU.  Method names follow the
-    reference; array arguments are numpy arrays ([n, 3] for vectors)."""
+    """The ``sapporo`` class (C++).  Method names follow the reference; array
+    arguments are numpy arrays ([n, 3] for vectors).  ``devices`` (a list of
+    device ids, ids may repeat) spreads the j round-robin over one handle per
+    entry, as ``sapporo::open(…, devices, len(devices), …)``; the default is
+    the one device ``device``."""
 
     def __init__(self, device: int = 0, order: int = FOURTH, precision: int = DOUBLESINGLE,
-                 n_pipes: int | None = None):
+                 n_pipes: int | None = None, devices=None):
         self.lib = load_library()
         self.h = self.lib.sapporo_c_new()
         if not self.h:
@@ -257,7 +263,12 @@ class Sapporo:
         if n_pipes:
             os.environ["SAPPORO_NPIPES"] = str(int(n_pipes))
         try:
-            _check(self.lib.sapporo_c_open(self.h, device, order, precision), "open")
+            if devices is None:
+                _check(self.lib.sapporo_c_open(self.h, device, order, precision), "open")
+            else:
+                ids = _i32(list(devices))
+                _check(self.lib.sapporo_c_open_devices(self.h, len(ids), ids if len(ids) else None,
+                                                       order, precision), "open")
         finally:
             if n_pipes:
                 if old is None:
@@ -265,6 +276,12 @@ class Sapporo:
                 else:
                     os.environ["SAPPORO_NPIPES"] = old
         self.dev = self.lib.sapporo_c_device(self.h)
+        self.devs = [self.lib.sapporo_c_device_at(self.h, k)
+                     for k in range(self.lib.sapporo_c_n_devices(self.h))]
+
+    def _one_device(self, what):
+        if len(self.devs) != 1:
+            raise SapporoError(f"{what} reads one device; this object drives {len(self.devs)}")
 
     def close(self):
         if self.h:
@@ -332,6 +349,7 @@ class Sapporo:
     def neighbour_counts(self, ni=None) -> np.ndarray:
         """Exact neighbour counts of the last force call (the lists hold at most
         NGB_PB ids; a count >= NGB_PB is an overflow)."""
+        self._one_device("neighbour_counts")
         ni = self._ni if ni is None else ni
         cnt = np.zeros(max(ni, 1), dtype=np.int32)
         self.results_ready()
@@ -343,6 +361,7 @@ class Sapporo:
         [ni, RES_STRIDE] doubles = acc[3], pot, jerk[3], snap[3], ds2 of the
         nearest neighbour (float value; 1e11 when none), its id (-1 when
         none).  The input of the multi-GPU combine (sum, min-loc)."""
+        self._one_device("raw_results")
         ni = self._ni if ni is None else ni
         p, n = C.c_void_p(), C.c_int()
         _check(self.lib.sapb_results(self.dev, C.byref(p), C.byref(n)), "results", self.dev)
@@ -354,6 +373,7 @@ class Sapporo:
     def neighbour_lists(self, ni=None):
         """Counts [ni] and lists [ni, NGB_PB] of the last force call (entries
         past min(count, NGB_PB) are undefined)."""
+        self._one_device("neighbour_lists")
         ni = self._ni if ni is None else ni
         cnt = np.zeros(max(ni, 1), dtype=np.int32)
         lst = np.zeros(max(ni, 1) * NGB_PB, dtype=np.int32)
@@ -362,6 +382,7 @@ class Sapporo:
         return cnt[:ni], lst.reshape(-1, NGB_PB)[:ni]
 
     def results_ready(self):
+        self._one_device("results_ready")
         p, n = C.c_void_p(), C.c_int()
         _check(self.lib.sapb_results(self.dev, C.byref(p), C.byref(n)), "results", self.dev)
 
@@ -386,30 +407,35 @@ class Sapporo:
             d[name] = o[3 + 3 * k: 6 + 3 * k].copy()
         return d
 
-    # lower level
+    # lower level (settings go to every device of the object)
     def set_launch(self, tpi=0, ip=0, nslices=0):
-        _check(self.lib.sapb_set_launch(self.dev, tpi, ip, nslices), "set_launch", self.dev)
+        for d in self.devs:
+            _check(self.lib.sapb_set_launch(d, tpi, ip, nslices), "set_launch", d)
 
     def set_spatial(self, mode=1, delta=0.0):
         """Spatial mode of the mixed-precision force calls: 0 off (address
         order, double-single difference for every pair), 1 on for calls of
         >= 2^29 pairs and >= 2048 i (default), 2 on for every call; far tiles use the
         single-float difference, accurate to `delta` (0: 1e-6)."""
-        _check(self.lib.sapb_set_spatial(self.dev, int(mode), float(delta)), "set_spatial",
-               self.dev)
+        for d in self.devs:
+            _check(self.lib.sapb_set_spatial(d, int(mode), float(delta)), "set_spatial", d)
 
     def set_near(self, factor=16.0):
         """Mixed precision: an i's share of a j tile holding a pair with
         ds2 < factor * eps2 is summed in FP64 (0: every pair in FP32)."""
-        _check(self.lib.sapb_set_near(self.dev, float(factor)), "set_near", self.dev)
+        for d in self.devs:
+            _check(self.lib.sapb_set_near(d, float(factor)), "set_near", d)
 
     def spatial_stats(self, reset=False):
         """(far, all) (warp, j tile) pairs of the spatial-mode calls since the
         last reset."""
-        f, a = C.c_ulonglong(), C.c_ulonglong()
-        _check(self.lib.sapb_spatial_stats(self.dev, C.byref(f), C.byref(a), int(reset)),
-               "spatial_stats", self.dev)
-        return f.value, a.value
+        far = total = 0
+        for d in self.devs:
+            f, a = C.c_ulonglong(), C.c_ulonglong()
+            _check(self.lib.sapb_spatial_stats(d, C.byref(f), C.byref(a), int(reset)),
+                   "spatial_stats", d)
+            far, total = far + f.value, total + a.value
+        return far, total
 
     def plan(self, ni, nj):
         t, i, s = C.c_int(), C.c_int(), C.c_int()
@@ -418,6 +444,7 @@ class Sapporo:
         return t.value, i.value, s.value
 
     def set_stream(self, stream_ptr: int | None):
+        self._one_device("set_stream")
         _check(self.lib.sapb_set_stream(self.dev, C.c_void_p(stream_ptr or 0)), "set_stream",
                self.dev)
 

@@ -25,6 +25,10 @@ int sapporo_c_open(sapporo_c *s, int device, int order, int precision) {
   int list[1] = {device};
   return s->obj.open("linked-in kernels", list, 1, order, precision);
 }
+int sapporo_c_open_devices(sapporo_c *s, int ndev, const int *devices, int order, int precision) {
+  if (!s || (ndev > 0 && !devices)) return SAPB_EINVAL;
+  return s->obj.open("linked-in kernels", const_cast<int *>(devices), ndev, order, precision);
+}
 int sapporo_c_close(sapporo_c *s) { return s ? s->obj.close() : SAPB_EINVAL; }
 int sapporo_c_get_n_pipes(sapporo_c *s) { return s ? s->obj.get_n_pipes() : 0; }
 int sapporo_c_set_time(sapporo_c *s, double ti) { return s ? s->obj.set_time(ti) : SAPB_EINVAL; }
@@ -104,5 +108,9 @@ int sapporo_c_retrieve_state(sapporo_c *s, int addr, double *out) {
 
 int sapporo_c_last_status(sapporo_c *s) { return s ? s->obj.last_status : SAPB_EINVAL; }
 struct sapb_dev *sapporo_c_device(sapporo_c *s) { return s ? s->obj.device_handle() : nullptr; }
+int sapporo_c_n_devices(sapporo_c *s) { return s ? s->obj.n_devices() : 0; }
+struct sapb_dev *sapporo_c_device_at(sapporo_c *s, int k) {
+  return s ? s->obj.device_handle(k) : nullptr;
+}
 
 }  // extern "C"

@@ -1,4 +1,5 @@
-// The `sapporo` class on top of the sapb_* C ABI (one GPU).
+// The `sapporo` class on top of the sapb_* C ABI, one device handle per
+// device given to open.
 //
 // Behaviour follows lib/src/sapporohostclass.cpp of the reference:
 //   - set_j_particle stages into host memory only; j travel to the GPU at the
@@ -9,10 +10,17 @@
 //   - nearest neighbour: taken only when ds2 < 1e10, nnbindex zeroed first,
 //     dsmin_i written only when taken (:722-775);
 //   - neighbour lists: overflow when a count reaches NGB_PB (:804-835),
-//     get_ngb_list copies and sorts (:837-880).
-// Deviations: fatal exits become error returns;
-// one GPU is used whatever the device list says; get_ngb_list never copies
-// more than NGB_PB entries and flags overflow when the count reaches NGB_PB.
+//     get_ngb_list copies and sorts (:837-880);
+//   - several devices: j address a on device a % G at a / G (:473-474), the
+//     first nj addresses split as nj / G plus one on the first nj % G devices
+//     (:687-691), the i broadcast, forces and potentials summed over the
+//     devices in device order, the nearest neighbour the closest over the
+//     devices, lists concatenated in device order (:749-799, :837-880).
+// Deviations: fatal exits become error returns; get_ngb_list never copies
+// more than NGB_PB entries of a device and flags overflow when a device's
+// count reaches NGB_PB; of nearest neighbours at the same distance on two
+// devices the lower id is taken (the rule inside one device), so the result
+// does not depend on the number of devices.
 #include "../../include/sapporohostclass.h"
 
 #include <algorithm>
@@ -54,7 +62,6 @@ sapporo::sapporo()
       predict(false),
       nj_updated(false),
       predJOnHost(false),
-      nstaged_(0),
       jcache_n_(0),
       dev_ni(0),
       nj_last_(0),
@@ -63,48 +70,74 @@ sapporo::sapporo()
 
 sapporo::~sapporo() { close(); }
 
+// lib/src/sapporohostclass.cpp:90-163: |nprocs| devices (all visible ones
+// when 0); ids from `devices` when nprocs > 0, else 0, 1, ... (the reference
+// lets the driver choose when nprocs < 0).  A device id may repeat: each
+// entry gets its own handle, stream and memory.
 int sapporo::open(std::string kernelFile, int *devices, int nprocs, int order, int precision) {
   (void)kernelFile;  // kernels are linked into the library
-  if (dev_) close();
+  if (!devs_.empty()) close();
   integrationOrder = order;
   integrationPrecision = precision;
-  int device = 0;
-  if (nprocs > 0 && devices) device = devices[0];
-  if (nprocs > 1 || nprocs < -1)
-    fprintf(stderr, "sapporo: %d devices requested; this library drives one GPU (device %d)\n",
-            nprocs < 0 ? -nprocs : nprocs, device);
+  int visible = 0;
+  if (sapb_device_count(&visible) != SAPB_OK) visible = 0;
+  int G = nprocs < 0 ? -nprocs : nprocs;
+  if (G == 0) G = std::max(visible, 1);
+  std::vector<int> ids((size_t)G);
+  for (int k = 0; k < G; k++)
+    ids[k] = (nprocs > 0 && devices) ? devices[k] : (visible > 0 ? k % visible : k);
   const char *np = getenv("SAPPORO_NPIPES");
   const int pipes = np ? atoi(np) : NPIPES;
-  const int rc = sapb_open(&dev_, device, order, precision, pipes, 16384);
-  last_status = rc;
-  if (rc != SAPB_OK) {
-    report("open", rc, nullptr);
-    dev_ = nullptr;
-    return rc;
+  for (int k = 0; k < G; k++) {
+    sapb_dev *d = nullptr;
+    const int rc = sapb_open(&d, ids[k], order, precision, pipes, 16384);
+    if (rc != SAPB_OK) {
+      fprintf(stderr, "sapporo: device %d (entry %d of %d): ", ids[k], k, G);
+      report("open", rc, nullptr);
+      close();
+      return last_status = rc;
+    }
+    devs_.push_back(d);
   }
-  sapb_info(dev_, nullptr, nullptr, &n_pipes, nullptr, nullptr);
+  last_status = 0;
+  dev_ = devs_[0];
+  n_pipes = INT_MAX;
+  for (sapb_dev *d : devs_) {
+    int p = 0;
+    sapb_info(d, nullptr, nullptr, &p, nullptr, nullptr);
+    n_pipes = std::min(n_pipes, p);
+  }
   nj_max = 16384;  // lib/src/sapporohostclass.cpp:161-162
   stage_slot_.assign(nj_max, -1);
   pred_time_.assign(nj_max, NAN);
-  staged_addr_.clear();
-  nstaged_ = 0;
+  staged_addr_.assign((size_t)G, std::vector<int>());
+  dev_nj_.assign((size_t)G, 0);
+  ngb_count_h_.assign((size_t)G, std::vector<int>());
+  ngb_list_h_.assign((size_t)G, std::vector<int>());
   predict = false;
   nj_updated = false;
   predJOnHost = false;
   ngb_fetched_ = false;
   dev_ni = 0;
+  nj_last_ = 0;
   if (verbose())
-    fprintf(stderr, "sapporo: opened device %d, order %d, precision %d, %d pipes\n", device,
-            order, precision, n_pipes);
+    for (int k = 0; k < G; k++)
+      fprintf(stderr, "sapporo: opened device %d (entry %d of %d), order %d, precision %d, %d pipes\n",
+              ids[k], k, G, order, precision, n_pipes);
   return 0;
 }
 
 int sapporo::close() {
-  if (dev_) {
-    sapb_close(dev_);
-    dev_ = nullptr;
-  }
+  for (sapb_dev *d : devs_) sapb_close(d);
+  devs_.clear();
+  dev_ = nullptr;
   return 0;
+}
+
+int sapporo::nj_on(int g, int nj) const {
+  // lib/src/sapporohostclass.cpp:687-691
+  const int G = ndev();
+  return nj / G + (g < nj % G ? 1 : 0);
 }
 
 int sapporo::get_n_pipes() { return n_pipes; }
@@ -123,16 +156,40 @@ int sapporo::set_no_time() {
 }
 
 void sapporo::increase_jMemory() {
-  // lib/src/sapporohostclass.cpp:560-583 (one device)
+  // lib/src/sapporohostclass.cpp:560-583: +10 %, rounded up to a multiple of
+  // the device count; each device holds nj_max / G
+  const int G = std::max(ndev(), 1);
   int temp = (int)(nj_max * 1.1);
-  temp = temp + 1;
+  temp = (temp / G + 1) * G;
   nj_max = temp;
   stage_slot_.resize(nj_max, -1);
   pred_time_.resize(nj_max, NAN);
-  if (dev_) {
-    const int rc = sapb_reserve_j(dev_, nj_max);
-    if (rc) report("reserve_j", rc, dev_);
+  for (sapb_dev *d : devs_) {
+    const int rc = sapb_reserve_j(d, nj_max / G);
+    if (rc) report("reserve_j", rc, d);
   }
+}
+
+// The staging record of `address` on its device (a new slot when the address
+// is not staged yet), with the local address and id to be written by the
+// caller; null with rc set when the staging cannot grow.
+double *sapporo::stage_record(int address, int &rc) {
+  const int G = ndev();
+  const int g = address % G;
+  int slot = stage_slot_[address];
+  if (slot < 0) {
+    slot = (int)staged_addr_[g].size();
+    stage_slot_[address] = slot;
+    staged_addr_[g].push_back(address);
+  }
+  double *base = sapb_j_stage(devs_[g], (int)staged_addr_[g].size());
+  if (!base) {
+    rc = SAPB_ENOMEM;
+    report("j staging", rc, devs_[g]);
+    return nullptr;
+  }
+  rc = 0;
+  return base + (size_t)slot * sapb_j_stage_stride(devs_[g]);
 }
 
 int sapporo::set_j_particle(int address, int id, double tj, double dtj, double mass,
@@ -140,7 +197,7 @@ int sapporo::set_j_particle(int address, int id, double tj, double dtj, double m
                             double snp[3], double crk[3], double eps) {
   (void)k18;
   (void)dtj;
-  if (!dev_) return last_status = SAPB_EINVAL;
+  if (devs_.empty()) return last_status = SAPB_EINVAL;
   if (address < 0) {
     fprintf(stderr, "sapporo::set_j_particle: negative address %d\n", address);
     return last_status = SAPB_EINVAL;
@@ -158,20 +215,10 @@ int sapporo::set_j_particle(int address, int id, double tj, double dtj, double m
       return last_status = SAPB_EINVAL;
     }
   }
-  int slot = stage_slot_[address];
-  if (slot < 0) {
-    slot = nstaged_++;
-    stage_slot_[address] = slot;
-    staged_addr_.push_back(address);
-  }
-  double *base = sapb_j_stage(dev_, nstaged_);
-  if (!base) {
-    report("j staging", SAPB_ENOMEM, dev_);
-    return last_status = SAPB_ENOMEM;
-  }
-  const int ss = sapb_j_stage_stride(dev_);
-  double *r = base + (size_t)slot * ss;
-  put_int_pair(&r[0], address, id);
+  int rc = 0;
+  double *r = stage_record(address, rc);
+  if (!r) return last_status = rc;
+  put_int_pair(&r[0], address / ndev(), id);
   r[1] = tj;
   r[2] = mass;
   for (int d = 0; d < 3; d++) {
@@ -221,7 +268,8 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
                              const double *mass, const double *x, const double *v,
                              const double *a, const double *jrk, const double *snp,
                              const double *crk, const double *eps) {
-  if (!dev_ || n < 0 || (n && (!address || !id || !mass || !x))) return last_status = SAPB_EINVAL;
+  if (devs_.empty() || n < 0 || (n && (!address || !id || !mass || !x)))
+    return last_status = SAPB_EINVAL;
   if (n == 0) return 0;
   // the address rules of set_j_particle, in the given order; on a bad address
   // nothing of this call is staged
@@ -244,30 +292,38 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
   }
   predJOnHost = false;
   nj_updated = true;
-  // slots, then one staging reservation and a tight fill
+  // slots, then one staging reservation per device and a tight fill
+  const int G = ndev();
   std::vector<int> slots((size_t)n);
   for (int k = 0; k < n; k++) {
     const int addr = address[k];
+    const int g = G == 1 ? 0 : addr % G;
     int slot = stage_slot_[addr];
     if (slot < 0) {
-      slot = nstaged_++;
+      slot = (int)staged_addr_[g].size();
       stage_slot_[addr] = slot;
-      staged_addr_.push_back(addr);
+      staged_addr_[g].push_back(addr);
     }
     slots[k] = slot;
   }
-  double *base = sapb_j_stage(dev_, nstaged_);
-  if (!base) {
-    report("j staging", SAPB_ENOMEM, dev_);
-    return last_status = SAPB_ENOMEM;
+  std::vector<double *> bases((size_t)G, nullptr);
+  for (int g = 0; g < G; g++) {
+    if (staged_addr_[g].empty()) continue;
+    bases[g] = sapb_j_stage(devs_[g], (int)staged_addr_[g].size());
+    if (!bases[g]) {
+      report("j staging", SAPB_ENOMEM, devs_[g]);
+      return last_status = SAPB_ENOMEM;
+    }
   }
-  const int ss = sapb_j_stage_stride(dev_);
+  const int ss = sapb_j_stage_stride(devs_[0]);
   const bool six = integrationOrder > FOURTH;
   const int *sl = slots.data();
+  double *const *bs = bases.data();
   parallel_chunks(n, [=](int k0, int k1) {
     for (int k = k0; k < k1; k++) {
-      double *r = base + (size_t)sl[k] * ss;
-      put_int_pair(&r[0], address[k], id[k]);
+      const int addr = address[k];
+      double *r = (G == 1 ? bs[0] : bs[addr % G]) + (size_t)sl[k] * ss;
+      put_int_pair(&r[0], G == 1 ? addr : addr / G, id[k]);
       r[1] = t ? t[k] : 0.0;
       r[2] = mass[k];
       for (int d = 0; d < 3; d++) {
@@ -288,24 +344,28 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
 }
 
 int sapporo::push_staged() {
-  if (!nj_updated || nstaged_ == 0) {
-    nj_updated = false;
-    return 0;
+  if (!nj_updated) return 0;
+  int rc = 0;
+  for (int g = 0; g < ndev(); g++) {
+    std::vector<int> &staged = staged_addr_[g];
+    if (staged.empty()) continue;
+    const int r = sapb_push_j(devs_[g], (int)staged.size());
+    for (int a : staged) {
+      stage_slot_[a] = -1;
+      pred_time_[a] = NAN;
+    }
+    staged.clear();
+    if (r) {
+      report("push_j", r, devs_[g]);
+      if (!rc) rc = r;
+    }
   }
-  const int rc = sapb_push_j(dev_, nstaged_);
-  for (int a : staged_addr_) {
-    stage_slot_[a] = -1;
-    pred_time_[a] = NAN;
-  }
-  staged_addr_.clear();
-  nstaged_ = 0;
   nj_updated = false;
-  if (rc) report("push_j", rc, dev_);
   return rc;
 }
 
 void sapporo::send_j_particles_to_device() {
-  if (dev_) last_status = push_staged();
+  if (!devs_.empty()) last_status = push_staged();
 }
 
 void sapporo::send_i_particles_to_device(int i) {
@@ -320,7 +380,7 @@ void sapporo::startGravCalc(int nj, int ni, int id[], double xi[][3], double vi[
   (void)eps2_i;  // stored by the reference (vel_i.w) but unused by its kernels
   last_status = 0;
   if (ni == 0 || nj == 0) return;
-  if (!dev_ || ni < 0 || nj < 0) {
+  if (devs_.empty() || ni < 0 || nj < 0) {
     last_status = SAPB_EINVAL;
     return;
   }
@@ -350,15 +410,33 @@ void sapporo::startGravCalc(int nj, int ni, int id[], double xi[][3], double vi[
       r[11] = 0.0;
     }
   }
-  int rc = push_staged();
-  if (!rc) {
-    int flags = SAPB_F_NGB_LIST;
-    if (predict) flags |= SAPB_F_PREDICT;
-    rc = sapb_force(dev_, nj, ni, eps2, t_i, flags);
-    if (!rc && predict)
-      for (int k = 0; k < nj && k < (int)pred_time_.size(); k++) pred_time_[k] = t_i;
+  // the same i on every device (lib/src/sapporohostclass.cpp:651-660)
+  int rc = 0;
+  for (int g = 1; g < ndev() && !rc; g++) {
+    double *copy = sapb_i_stage(devs_[g], ni);
+    if (!copy) {
+      rc = SAPB_ENOMEM;
+      report("i staging", rc, devs_[g]);
+    } else {
+      memcpy(copy, rec, sizeof(double) * (size_t)ni * is);
+    }
   }
-  if (rc) report("startGravCalc", rc, dev_);
+  if (!rc) rc = push_staged();
+  int flags = SAPB_F_NGB_LIST;
+  if (predict) flags |= SAPB_F_PREDICT;
+  for (int g = 0; g < ndev(); g++) dev_nj_[g] = 0;
+  for (int g = 0; g < ndev() && !rc; g++) {
+    const int njg = nj_on(g, nj);
+    if (njg == 0) continue;  // no j on this device: it adds nothing
+    rc = sapb_force(devs_[g], njg, ni, eps2, t_i, flags);
+    if (rc) {
+      report("startGravCalc", rc, devs_[g]);
+    } else {
+      dev_nj_[g] = njg;
+    }
+  }
+  if (!rc && predict)
+    for (int k = 0; k < nj && k < (int)pred_time_.size(); k++) pred_time_[k] = t_i;
   last_status = rc;
   dev_ni = ni;
   nj_last_ = nj;
@@ -382,90 +460,121 @@ int sapporo::getGravResults(int nj, int ni, int index[], double xi[][3], double 
       if (crk) crk[i][0] = crk[i][1] = crk[i][2] = 0;
     }
   }
-  if (!dev_) return last_status = SAPB_EINVAL;
+  if (devs_.empty()) return last_status = SAPB_EINVAL;
   if (last_status) return last_status;
-  const double *res = nullptr;
-  int nres = 0;
-  const int rc = sapb_results(dev_, &res, &nres);
-  if (rc) {
-    report("getGravResults", rc, dev_);
-    return last_status = rc;
-  }
-  const int n = std::min(ni, nres);
-  for (int i = 0; i < n; i++) {
-    const double *r = res + (size_t)i * SAPB_RES_STRIDE;
-    acc[i][0] += r[0];
-    acc[i][1] += r[1];
-    acc[i][2] += r[2];
-    pot[i] += r[3];
-    if (integrationOrder > GRAPE5) {
-      jerk[i][0] += r[4];
-      jerk[i][1] += r[5];
-      jerk[i][2] += r[6];
-      if (ngb) {
-        const double ds = r[10];
-        if (ds < 1.0e10) {  // lib/src/sapporohostclass.cpp:732, 767-774
-          nnbindex[i] = (int)r[11];
-          if (dsmin_i) dsmin_i[i] = ds;
+  // nearest neighbour over the devices: ds2 < 1e10 (lib/src/sapporohostclass.cpp:732,
+  // 767-774), the lower id at equal ds2
+  std::vector<double> best_ds(ngb ? (size_t)ni : 0, 1.0e10);
+  for (int g = 0; g < ndev(); g++) {
+    if (dev_nj_[g] == 0) continue;
+    const double *res = nullptr;
+    int nres = 0;
+    const int rc = sapb_results(devs_[g], &res, &nres);
+    if (rc) {
+      report("getGravResults", rc, devs_[g]);
+      return last_status = rc;
+    }
+    const int n = std::min(ni, nres);
+    for (int i = 0; i < n; i++) {
+      const double *r = res + (size_t)i * SAPB_RES_STRIDE;
+      acc[i][0] += r[0];
+      acc[i][1] += r[1];
+      acc[i][2] += r[2];
+      pot[i] += r[3];
+      if (integrationOrder > GRAPE5) {
+        jerk[i][0] += r[4];
+        jerk[i][1] += r[5];
+        jerk[i][2] += r[6];
+        if (ngb) {
+          const double ds = r[10];
+          const int id = (int)r[11];
+          if (ds < best_ds[i] ||
+              (ds == best_ds[i] && ds < 1.0e10 && (unsigned)id < (unsigned)nnbindex[i])) {
+            best_ds[i] = ds;
+            nnbindex[i] = id;
+            if (dsmin_i) dsmin_i[i] = ds;
+          }
         }
       }
-    }
-    if (integrationOrder > FOURTH) {
-      snp[i][0] += r[7];
-      snp[i][1] += r[8];
-      snp[i][2] += r[9];
+      if (integrationOrder > FOURTH) {
+        snp[i][0] += r[7];
+        snp[i][1] += r[8];
+        snp[i][2] += r[9];
+      }
     }
   }
   return 0;
 }
 
 int sapporo::fetch_ngb_list_from_device(int) {
-  if (!dev_) return 0;
-  ngb_count_h_.resize((size_t)std::max(dev_ni, 1));
-  ngb_list_h_.resize((size_t)std::max(dev_ni, 1) * NGB_PB);
-  const double *res = nullptr;
-  sapb_results(dev_, &res, nullptr);  // the lists belong to the last force call
-  const int rc = sapb_ngb_fetch(dev_, ngb_count_h_.data(), ngb_list_h_.data(), dev_ni);
-  if (rc) {
-    report("ngb fetch", rc, dev_);
-    return 0;
+  if (devs_.empty()) return 0;
+  const size_t n = (size_t)std::max(dev_ni, 1);
+  for (int g = 0; g < ndev(); g++) {
+    std::vector<int> &cnt = ngb_count_h_[g];
+    std::vector<int> &lst = ngb_list_h_[g];
+    cnt.assign(n, 0);
+    lst.resize(n * NGB_PB);
+    if (dev_nj_[g] == 0) continue;  // no j on this device: no neighbours
+    const double *res = nullptr;
+    sapb_results(devs_[g], &res, nullptr);  // the lists belong to the last force call
+    const int rc = sapb_ngb_fetch(devs_[g], cnt.data(), lst.data(), dev_ni);
+    if (rc) {
+      report("ngb fetch", rc, devs_[g]);
+      return 0;
+    }
   }
   ngb_fetched_ = true;
   return dev_ni;
 }
 
 int sapporo::read_ngb_list(int cluster_id) {
+  // lib/src/sapporohostclass.cpp:804-835: overflow when a device's count
+  // reaches NGB_PB
   const int ni = fetch_ngb_list_from_device(cluster_id);
   bool overflow = false;
-  for (int j = 0; j < ni; j++)
-    if (ngb_count_h_[j] >= NGB_PB) overflow = true;
+  for (int g = 0; g < ndev() && ni > 0; g++)
+    for (int j = 0; j < ni; j++)
+      if (ngb_count_h_[g][j] >= NGB_PB) overflow = true;
   return overflow;
 }
 
 int sapporo::get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, int nbl[]) {
+  // lib/src/sapporohostclass.cpp:837-880: the devices' lists in device order,
+  // overflow once the total reaches maxlength; then sorted
   nblen = 0;
   if (!ngb_fetched_) fetch_ngb_list_from_device(cluster_id);
   if (ipipe < 0 || ipipe >= dev_ni || !ngb_fetched_) return 1;
-  const int len = ngb_count_h_[ipipe];
-  const int to_copy = std::max(0, std::min(std::min(len, maxlength), NGB_PB));
-  memcpy(nbl, &ngb_list_h_[(size_t)ipipe * NGB_PB], sizeof(int) * to_copy);
-  nblen = len;
-  const bool overflow = nblen >= maxlength || len >= NGB_PB;
-  std::sort(nbl, nbl + to_copy);
+  bool overflow = false;
+  int copied = 0;
+  for (int g = 0; g < ndev(); g++) {
+    const int len = ngb_count_h_[g][ipipe];
+    const int to_copy = std::max(0, std::min(std::min(len, NGB_PB), maxlength - copied));
+    memcpy(nbl + copied, &ngb_list_h_[g][(size_t)ipipe * NGB_PB], sizeof(int) * to_copy);
+    copied += to_copy;
+    nblen += len;
+    if (len >= NGB_PB) overflow = true;  // ids beyond NGB_PB were not stored
+    if (nblen >= maxlength) {
+      overflow = true;
+      break;
+    }
+  }
+  std::sort(nbl, nbl + copied);
   if (overflow && verbose())
     fprintf(stderr, "sapporo::get_ngb_list(..) - overflow for ipipe= %d, ngb= %d\n", ipipe, nblen);
   return overflow;
 }
 
 void sapporo::forcePrediction(int nj) {
-  if (!dev_) return;
+  if (devs_.empty()) return;
   int rc = push_staged();
-  if (!rc && predict && nj > 0) {
-    rc = sapb_predict(dev_, nj, t_i);
-    if (!rc)
-      for (int k = 0; k < nj && k < (int)pred_time_.size(); k++) pred_time_[k] = t_i;
+  for (int g = 0; g < ndev() && !rc && predict && nj > 0; g++) {
+    const int njg = nj_on(g, nj);
+    if (njg == 0) continue;
+    rc = sapb_predict(devs_[g], njg, t_i);
+    if (rc) report("forcePrediction", rc, devs_[g]);
   }
-  if (rc) report("forcePrediction", rc, dev_);
+  if (!rc && predict && nj > 0)
+    for (int k = 0; k < nj && k < (int)pred_time_.size(); k++) pred_time_[k] = t_i;
   last_status = rc;
   predict = false;
 }
@@ -475,16 +584,36 @@ void sapporo::forcePrediction(int nj) {
 // of the most recent prediction; addresses pushed after that prediction or
 // predicted at an older time are handled one by one.
 int sapporo::refresh_jcache(int addr) {
-  if (!dev_) return SAPB_EINVAL;
+  if (devs_.empty() || addr < 0) return SAPB_EINVAL;
+  const int G = ndev();
   int cap = 0;
-  sapb_info(dev_, nullptr, nullptr, nullptr, &cap, nullptr);
-  if (addr < 0 || addr >= cap) return SAPB_EINVAL;
+  sapb_info(devs_[addr % G], nullptr, nullptr, nullptr, &cap, nullptr);
+  if (addr / G >= cap) return SAPB_EINVAL;
   if (!predJOnHost) {
     push_staged();
-    const int n = std::min(cap, nj_max);
-    jcache_.resize((size_t)n * 24);
-    const int rc = sapb_read_j(dev_, 0, n, t_i, 1, jcache_.data());
-    if (rc) return rc;
+    // all addresses below nj_max that the devices hold, device by device
+    std::vector<int> caps((size_t)G, 0);
+    int n = 0;
+    for (int g = 0; g < G; g++) {
+      sapb_info(devs_[g], nullptr, nullptr, nullptr, &caps[g], nullptr);
+      n = std::max(n, std::min(nj_max, caps[g] * G));
+    }
+    jcache_.assign((size_t)n * 24, 0.0);
+    std::vector<double> part;
+    for (int g = 0; g < G; g++) {
+      const int ng = std::min(caps[g], n > g ? (n - g + G - 1) / G : 0);
+      if (ng == 0) continue;
+      double *out = jcache_.data();
+      if (G > 1) {
+        part.resize((size_t)ng * 24);
+        out = part.data();
+      }
+      const int rc = sapb_read_j(devs_[g], 0, ng, t_i, 1, out);
+      if (rc) return rc;
+      if (G > 1)
+        for (int la = 0; la < ng; la++)
+          memcpy(&jcache_[(size_t)(la * G + g) * 24], &part[(size_t)la * 24], 24 * sizeof(double));
+    }
     jcache_n_ = n;
     predJOnHost = true;
   }
@@ -492,7 +621,8 @@ int sapporo::refresh_jcache(int addr) {
   const double pt = addr < (int)pred_time_.size() ? pred_time_[addr] : NAN;
   if (std::isnan(pt) || pt != t_i) {
     double one[24];
-    const int rc = sapb_read_j(dev_, addr, 1, std::isnan(pt) ? 0.0 : pt, std::isnan(pt) ? 0 : 1, one);
+    const int rc = sapb_read_j(devs_[addr % G], addr / G, 1, std::isnan(pt) ? 0.0 : pt,
+                               std::isnan(pt) ? 0 : 1, one);
     if (rc) return rc;
     memcpy(&jcache_[(size_t)addr * 24], one, sizeof one);
   }

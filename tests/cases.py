@@ -54,13 +54,14 @@ def oracle_force(case: dict, sel=None, lists=True) -> dict:
 
 
 def run_library(case: dict, precision: int, sel=None, lists=True, launch=None,
-                spatial=None) -> dict:
+                spatial=None, devices=None) -> dict:
     """Drives the sapporo class exactly as an integrator would: stage all j,
     set_time, startGravCalc on the selected i, getGravResults, neighbour
-    readout.  `spatial` = (mode, delta) sets the spatial mode first."""
+    readout.  `spatial` = (mode, delta) sets the spatial mode first;
+    `devices` = a device list for open (the j spread over its entries)."""
     import sapporo2_b200 as sp
     o, n = case["order"], case["n"]
-    with sp.Sapporo(order=o, precision=precision) as s:
+    with sp.Sapporo(order=o, precision=precision, devices=devices) as s:
         if launch:
             s.set_launch(*launch)
         if spatial is not None:
@@ -73,7 +74,8 @@ def run_library(case: dict, precision: int, sel=None, lists=True, launch=None,
                 case["pa"][idx] if case["pa"] is not None else None, case["eps2"],
                 case["h2"][idx])
         r = s.results(n, ngb=True)
-        r["raw"] = s.raw_results(len(idx)).copy()
+        if devices is None:
+            r["raw"] = s.raw_results(len(idx)).copy()
         if spatial is not None:
             r["far_tiles"] = s.spatial_stats()  # (far, all) (warp, tile) pairs
         if lists:

@@ -21,9 +21,14 @@ def test_fp64_kernel_matches_oracle(gpu, order):
     print(st)
 
 
+@pytest.mark.parametrize("eps2", [1e-6, 0.0])
 @pytest.mark.parametrize("order", [1, 2])
-def test_mixed_kernel_matches_oracle(gpu, order):
-    case = T.build_case(order, 2048, seed=12, binaries=0.1)
+def test_mixed_kernel_matches_oracle(gpu, order, eps2):
+    """Softened and unsoftened (eps2 = 0: no near-pair FP64 sums, binaries
+    1e-6..1e-4 apart in plain double-single arithmetic).  Unsoftened, the j
+    are given at t_i: a Taylor step of up to 7/1024 along the orbits of such
+    binaries (accelerations ~1e9) would throw them far out of the system."""
+    case = T.build_case(order, 2048, seed=12, binaries=0.1, eps2=eps2, t_spread=eps2 > 0)
     want = T.oracle_force(case)
     got = T.run_library(case, sp.DOUBLESINGLE)
     st = T.check_forces(got, want, order)
@@ -100,3 +105,12 @@ def test_fp64_kernel_rsqrt_over_scales(gpu, eps2):
     ea = np.linalg.norm(got["acc"] - acc, axis=1) / np.linalg.norm(acc, axis=1)
     ep = np.abs(got["pot"] - pot) / np.abs(pot)
     assert ea.max() < 2e-15 and ep.max() < 1e-15, (ea.max(), ep.max())
+
+
+def test_near_pair_factor_is_checked(gpu):
+    with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
+        for bad in (-1.0, float("nan"), 2e6):
+            with pytest.raises(sp.SapporoError):
+                s.set_near(bad)
+        s.set_near(0.0)
+        s.set_near(64.0)

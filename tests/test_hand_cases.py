@@ -1,8 +1,9 @@
 """GPU: hand-made cases with known answers, through the sapporo class --
 two bodies against the closed form, a binary 1e-6 apart at unit radius (the
 reason the position difference is double-single), a j exactly on the h2
-boundary (the list test is strict: h2 > ds2), and neighbour counts of 255,
-256 and 257 (overflow from 256 on)."""
+boundary (the list test is strict: h2 > ds2), neighbour counts of 255,
+256 and 257 (overflow from 256 on), and a softened pair next to the zero of
+its snap (the reason close pairs are summed in FP64)."""
 import numpy as np
 import pytest
 
@@ -106,3 +107,48 @@ def test_neighbour_overflow_at_256(gpu, prec, k):
     else:  # the list holds 256 of the k, all genuine neighbours
         assert len(ids) == 256 and len(set(ids)) == 256 and ids.max() < n_in
     assert r["nnb"][0] == int(np.argmin(rad))
+
+
+def _snap_pair(xj, vj, aj, mj, xi, vi, ai, eps2):
+    """Snap of one softened pair, in FP64 (kernels.cu:642-667)."""
+    dr, dv, da = (np.subtract(q, p) for q, p in ((xj, xi), (vj, vi), (aj, ai)))
+    r2 = dr @ dr + eps2
+    inv3 = r2 ** -1.5
+    al = (dr @ dv) / r2
+    be = (dv @ dv + dr @ da) / r2 + al * al
+    jij = mj * inv3 * dv - 3 * al * mj * inv3 * dr
+    return mj * inv3 * da - 6 * al * jij - 3 * be * mj * inv3 * dr
+
+
+@pytest.mark.parametrize("near", [16.0, 0.0])
+def test_softened_pair_near_its_snap_zero(gpu, near):
+    """Two bodies receding radially from each other at r^2 = 1.5 eps^2 (1 +
+    1e-4), just off the separation where the radial snap of a softened pair
+    vanishes (6 r^2 = 9 eps^2): the snap is 3e-4 of its scale there, so FP32
+    rounding of the pair's terms alone is a ~2e-3 relative error.  The FP64
+    near-pair sum (default factor 16: pairs within 4 softening lengths) keeps
+    it near 1e-8 (the FP32 rounding of the stored mass); with the factor 0
+    (every pair in FP32, as the reference's double-single kernels) it is
+    above 1e-4.  One of the two is at unit radius, like a cluster particle."""
+    eps2 = 1e-6
+    r = np.sqrt(1.5 * eps2 * (1 + 1e-4))
+    x = np.array([[1.0, 0.0, 0.0], [1.0 + r, 0.0, 0.0]])
+    # velocities exact in FP32, so the records' rounding does not enter
+    v = np.array([[0.25, 0.0, 0.0], [1.25, 0.0, 0.0]])
+    m = np.array([1e-6, 1e-6])
+    z = np.zeros((2, 3))
+    with sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE) as s:
+        s.set_near(near)
+        s.set_j_particles(np.arange(2), np.arange(2), np.zeros(2), m, x, v, z, z, z, z)
+        s.set_time(0.0)
+        s.start(2, np.arange(2), x, v, z, eps2, np.zeros(2))
+        got = s.results(2)
+    for i, j in ((0, 1), (1, 0)):
+        want = _snap_pair(x[j], v[j], z[j], m[j], x[i], v[i], z[i], eps2)
+        scale = m[j] * (r * r + eps2) ** -1.5 / np.sqrt(r * r + eps2)  # |dv| = 1
+        err = np.linalg.norm(got["snp"][i] - want) / np.linalg.norm(want)
+        print(f"near {near}: |snap| / scale = {np.linalg.norm(want) / scale:.1e}, rel err {err:.2e}")
+        if near > 0:
+            assert err < 1e-5
+        else:
+            assert err > 1e-4
