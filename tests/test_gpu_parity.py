@@ -9,13 +9,17 @@ from tests import cases as T
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("eps2", [1e-6, 0.0])
 @pytest.mark.parametrize("order", [1, 2])
-def test_fp64_kernel_matches_oracle(gpu, order):
-    case = T.build_case(order, 2048, seed=11, binaries=0.1)
+def test_fp64_kernel_matches_oracle(gpu, order, eps2):
+    case = T.build_case(order, 2048, seed=11, binaries=0.1, eps2=eps2, t_spread=eps2 > 0)
     want = T.oracle_force(case)
     got = T.run_library(case, sp.DOUBLE)
-    # all-FP64 kernel: only summation order and rsqrt rounding differ
-    st = T.check_forces(got, want, order, median_tol=1e-13, max_tol=1e-9)
+    # all-FP64 kernel: only summation order and rsqrt rounding differ.  The
+    # unsoftened snap is ill-conditioned (each binary's two a_j ~5e8 cancel):
+    # the oracle summed in two j orders differs by 4e-11 median, 5e-9 max
+    med, mx = (1e-13, 1e-9) if eps2 > 0 else (1e-9, 1e-7)
+    st = T.check_forces(got, want, order, median_tol=med, max_tol=mx)
     assert T.check_nn(case, got["nnb"], want) == 0
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want)
     print(st)
@@ -27,11 +31,21 @@ def test_mixed_kernel_matches_oracle(gpu, order, eps2):
     """Softened and unsoftened (eps2 = 0: no near-pair FP64 sums, binaries
     1e-6..1e-4 apart in plain double-single arithmetic).  Unsoftened, the j
     are given at t_i: a Taylor step of up to 7/1024 along the orbits of such
-    binaries (accelerations ~1e9) would throw them far out of the system."""
+    binaries (accelerations ~5e8) would throw them far out of the system.
+
+    Unsoftened 6th order is checked without snap: the snap of every i sums
+    m r^-3 (a_j - a_i) over each binary's two members, whose accelerations
+    (~5e8, opposite) cancel; taken in FP32, as the reference's sixth_DS
+    kernel takes them too (kernels.cu:642-644, Tvel = float), their rounding
+    (~15 per component) leaves a snap error of ~1e-2 relative.  That case
+    needs the FP64 kernels (the reference's 6th-order interface defaults to
+    them, sapporo6thlib.cpp:29), which test_fp64_kernel_matches_oracle
+    checks at eps2 = 0."""
     case = T.build_case(order, 2048, seed=12, binaries=0.1, eps2=eps2, t_spread=eps2 > 0)
     want = T.oracle_force(case)
     got = T.run_library(case, sp.DOUBLESINGLE)
-    st = T.check_forces(got, want, order)
+    fields = ["acc", "pot", "jrk"] if (order == 2 and eps2 == 0) else None
+    st = T.check_forces(got, want, order, fields=fields)
     T.check_nn(case, got["nnb"], want)
     T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], want)
     print(st)
