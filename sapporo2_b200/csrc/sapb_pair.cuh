@@ -291,14 +291,14 @@ __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, cons
 // low part is below 2^-24 |x|): 3 FMA-pipe operations instead of 9, and the
 // softening enters the first FMA of the squared distance (one operation
 // less; no pair of a far tile is a nearest neighbour, so its unsoftened ds2
-// is not needed: the caller checks that against the i's bounds).  With LIST
-// the minimum of this approximate softened ds2 is kept so the caller can
-// rescan the tile exactly for list members.  The self pair is still masked
-// by id.
-template <int ORDER, bool LIST>
+// is not needed: the caller checks that against the i's bounds).  No
+// distance minimum is kept either: the caller rescans a far tile for list
+// members when the tile's box comes within h2 of the i.  The self pair is
+// still masked by id.
+template <int ORDER>
 __device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, const float4 &r1,
                                               const float4 &r2, const float4 &r3, float2 eps2,
-                                              AccMix2 &A, float2 &tmin) {
+                                              AccMix2 &A) {
   Pre2 P;
   P.dx = __fadd2_rn(bc2(r0.x), I.nxh);
   P.dy = __fadd2_rn(bc2(r0.y), I.nyh);
@@ -309,10 +309,6 @@ __device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, 
     P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
   }
   const float2 r2v = __ffma2_rn(P.dz, P.dz, __ffma2_rn(P.dy, P.dy, __ffma2_rn(P.dx, P.dx, eps2)));
-  if (LIST) {
-    tmin.x = fminf(tmin.x, r2v.x);
-    tmin.y = fminf(tmin.y, r2v.y);
-  }
   P.inv = make_float2(rsqrt_mufu(r2v.x), rsqrt_mufu(r2v.y));
   pair_mix2_post<ORDER>(I, P, r0.w, r2, r3, A);
 }
