@@ -192,6 +192,9 @@ __global__ void __launch_bounds__(256) ikey_kernel(const double *__restrict__ ir
 // minimum (the force kernel's double-single ds2, self pair masked by id) over
 // the j tile whose key range holds the i key -- the last tile whose first
 // key is <= it, tile 0 if none -- i.e. over spatial neighbours of the i.
+// One warp per i: the lanes take every 32nd record of the tile (coalesced)
+// and the minimum is reduced across the warp.
+constexpr int kBoundWarps = 8;  // i per 256-thread block
 template <int RS>
 __global__ void __launch_bounds__(256) bound_kernel(const double *__restrict__ irec, int istride,
                                                     const int *__restrict__ iperm,
@@ -199,8 +202,9 @@ __global__ void __launch_bounds__(256) bound_kernel(const double *__restrict__ i
                                                     const float4 *__restrict__ spred, int nj,
                                                     const unsigned *__restrict__ tkey,
                                                     float *bound) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ni) return;
+  const int lane = threadIdx.x & 31;
+  const int g = blockIdx.x * kBoundWarps + (threadIdx.x >> 5);
+  if (g >= ni) return;  // the whole warp
   const int ntiles = (nj + kTJ - 1) / kTJ;
   const unsigned k = ikey[g];
   int lo = 0, hi = ntiles;  // first tile with tkey > k lies in [lo, hi]
@@ -222,12 +226,12 @@ __global__ void __launch_bounds__(256) bound_kernel(const double *__restrict__ i
   const int cnt = min(kTJ, nj - t * kTJ);
   const float4 *rec = spred + (size_t)t * kTJ * RS;
   float m = FLT_MAX;
-#pragma unroll 4
-  for (int q = 0; q < cnt; q++) {
+  for (int q = lane; q < cnt; q += 32) {
     float dx, dy, dz;
     m = fminf(m, pair_dr_mix(I, rec[q * RS + 0], rec[q * RS + 1], dx, dy, dz));
   }
-  bound[g] = m;
+  for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) bound[g] = m;
 }
 
 }  // namespace sapb
@@ -387,12 +391,13 @@ int spatial_prepare(sapb_dev *d, int nj, int ni, const double *i_dev) {
   if (e == cudaSuccess) {
     const int is = i_stride(d->order);
     const float4 *sp4 = static_cast<const float4 *>(S.spred);
+    const int nb = (ni + kBoundWarps - 1) / kBoundWarps;
     if (rs == 4)
-      bound_kernel<4><<<(ni + 255) / 256, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, sp4,
-                                                        nj, S.tkey, S.ibound);
+      bound_kernel<4><<<nb, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, sp4, nj, S.tkey,
+                                          S.ibound);
     else
-      bound_kernel<3><<<(ni + 255) / 256, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, sp4,
-                                                        nj, S.tkey, S.ibound);
+      bound_kernel<3><<<nb, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, sp4, nj, S.tkey,
+                                          S.ibound);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess)
