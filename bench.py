@@ -727,9 +727,9 @@ def spatial_mode() -> int:
 
 def spatial_on(ni: int, nj: int) -> bool:
     """Whether a mixed-precision force call of ni x nj pairs runs in spatial
-    mode (the library's rule: mode 2, or mode 1, >= 2048 i and >= 2^29 pairs)."""
+    mode (the library's rule: mode 2, or mode 1, >= 1024 i and >= 2^28 pairs)."""
     m = spatial_mode()
-    return m == 2 or (m == 1 and ni >= 2048 and nj >= 1024 and ni * nj >= 1 << 29)
+    return m == 2 or (m == 1 and ni >= 1024 and nj >= 1024 and ni * nj >= 1 << 28)
 
 
 def main():

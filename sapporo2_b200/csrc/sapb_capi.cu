@@ -522,12 +522,13 @@ double *sapb_i_stage(sapb_dev *d, int ni) {
 }
 
 // Spatial mode pays for its per-call work (the i sort and bounds, the j
-// gather after each prediction) from about 2^29 pairs and 2048 i on (B200,
-// predict + force per call, i a random subset of the j: 1.00-1.03 x from 2^29
-// to 2^31, 1.06-1.08 x from 2^33; block-step active sets, which are spatially
-// clustered, gain more); smaller calls run in address order.
-constexpr double kSpatialMinPairs = 536870912.0;  // 2^29
-constexpr int kSpatialMinI = 2048;
+// gather after each prediction) from about 2^28 pairs and 1024 i on (B200,
+// predict + force per call, neighbour lists on, i a random subset of the j:
+// 1.04-1.05 x at 2^28 to 2^30, 1.07-1.12 x from 2^31; 0.91 and 1.00 x at 2^26
+// and 2^27; block-step active sets, which are spatially clustered, gain
+// more); smaller calls run in address order.
+constexpr double kSpatialMinPairs = 268435456.0;  // 2^28
+constexpr int kSpatialMinI = 1024;
 
 static bool use_spatial(const sapb_dev *d, int ni, int nj) {
   if (d->prec != DOUBLESINGLE || d->sp.mode == 0) return false;
