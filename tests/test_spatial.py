@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 import sapporo2_b200 as sp
+from sapporo2_b200 import ic
 from tests import cases as T
 
 pytestmark = pytest.mark.gpu
@@ -166,6 +167,26 @@ def test_spatial_default_mode_threshold(gpu):
     got = T.run_library(case, sp.DOUBLESINGLE, spatial=(1, 0.0))
     ref = T.run_library(case, sp.DOUBLESINGLE, spatial=(0, 0.0))
     assert np.array_equal(got["raw"], ref["raw"])
+
+
+def test_spatial_default_mode_turns_on_at_threshold(gpu):
+    """Mode 1 orders a call from 2^28 pairs and 1024 i on: 1023 i x 2^18 j
+    runs in address order, 1024 i x 2^18 j (2^28 pairs) in spatial mode."""
+    n = 1 << 18
+    x, v, m = ic.plummer(n, 27)
+    z = np.zeros((n, 3))
+    ids = np.arange(n, dtype=np.int32)
+    with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
+        s.set_spatial(1, 0.0)
+        s.set_j_particles(np.arange(n), ids, np.zeros(n), m, x, v, z, z, z, z)
+        s.set_time(0.0)
+        for ni, on in ((1023, False), (1024, True)):
+            sel = (np.arange(ni) * 257) % n
+            s.start(n, ids[sel], x[sel], v[sel], z[sel], 1e-6, np.zeros(ni))
+            r = s.results(n)
+            assert np.all(np.isfinite(r["acc"]))
+            far, tiles = s.spatial_stats(reset=True)
+            assert (tiles > 0) == on, (ni, far, tiles)
 
 
 def test_spatial_rejects_bad_arguments(gpu):
