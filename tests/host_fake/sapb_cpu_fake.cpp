@@ -45,6 +45,7 @@ struct sapb_dev {
 
 namespace {
 int g_pushes = 0;  // pushes over all devices (the test reads it through fake_sapb_pushes)
+std::vector<sapb_dev *> g_open;  // handles open now, in the order they were opened
 
 int ndevices() {
   const char *e = getenv("FAKE_SAPB_DEVICES");
@@ -77,6 +78,13 @@ extern "C" {
 
 int fake_sapb_pushes(void) { return g_pushes; }
 
+// Device ids of the handles open now (up to max of them); returns their number.
+int fake_sapb_open_devices(int *ids, int max) {
+  const int n = (int)g_open.size();
+  for (int k = 0; k < n && k < max; k++) ids[k] = g_open[k]->device;
+  return n;
+}
+
 const char *sapb_error_string(int code) {
   switch (code) {
     case SAPB_OK: return "ok";
@@ -102,11 +110,13 @@ int sapb_open(sapb_dev **out, int device, int order, int precision, int n_pipes,
   d->prec = precision;
   d->n_pipes = n_pipes > 0 ? n_pipes : SAPB_NPIPES;
   grow(d, nj_reserve > 0 ? nj_reserve : 16384);
+  g_open.push_back(d);
   *out = d;
   return SAPB_OK;
 }
 
 int sapb_close(sapb_dev *d) {
+  g_open.erase(std::remove(g_open.begin(), g_open.end(), d), g_open.end());
   delete d;
   return SAPB_OK;
 }

@@ -46,6 +46,8 @@ def fake(tmp_path_factory):
             f = getattr(lib, name)
             f.restype, f.argtypes = res, args
     lib.fake_sapb_pushes.restype = C.c_int
+    lib.fake_sapb_open_devices.restype = C.c_int
+    lib.fake_sapb_open_devices.argtypes = [C.POINTER(C.c_int), C.c_int]
     return lib
 
 
@@ -249,6 +251,23 @@ def test_g6_interface_over_devices(fake):
     small = want["ngb_count"] < sp.NGB_PB
     np.testing.assert_array_equal(np.array([q[1] for q in lists])[small],
                                   want["ngb_count"][small])
+
+
+def test_g6_open_reads_the_device_list(fake, tmp_path, monkeypatch):
+    # ./sapporo2.config: the device count, then one id per line
+    # (lib/interfaces/sapporoG6lib.cpp:46-77); g6_open_ opens those devices
+    (tmp_path / "sapporo2.config").write_text("2\n0\n3\n")
+    monkeypatch.chdir(tmp_path)
+    g6 = sp.G6.__new__(sp.G6)
+    g6.lib = fake
+    assert g6.open() == 0
+    try:
+        ids = np.zeros(8, dtype=np.int32)
+        n = fake.fake_sapb_open_devices(ids.ctypes.data_as(C.POINTER(C.c_int)), 8)
+        assert list(ids[:n]) == [0, 3]
+    finally:
+        g6.close()
+    assert fake.fake_sapb_open_devices(ids.ctypes.data_as(C.POINTER(C.c_int)), 8) == 0
 
 
 def test_device_lists_and_readback(fake):
