@@ -192,19 +192,22 @@ __global__ void __launch_bounds__(256) ikey_kernel(const double *__restrict__ ir
 // minimum (the force kernel's double-single ds2, self pair masked by id) over
 // the j tile whose key range holds the i key -- the last tile whose first
 // key is <= it, tile 0 if none -- i.e. over spatial neighbours of the i.
-// One warp per i: the lanes take every 32nd record of the tile (coalesced)
-// and the minimum is reduced across the warp.
-constexpr int kBoundWarps = 8;  // i per 256-thread block
+// 2^lg lanes per i (1..32, aligned groups within a warp): the lanes take
+// every 2^lg-th record of the tile and the minimum is reduced across the
+// group.  Small calls take 32 lanes per i to fill the GPU; calls with enough
+// i for one thread each take one (the whole warp then reads one tile).
 template <int RS>
 __global__ void __launch_bounds__(256) bound_kernel(const double *__restrict__ irec, int istride,
                                                     const int *__restrict__ iperm,
                                                     const unsigned *__restrict__ ikey, int ni,
-                                                    const float4 *__restrict__ spred, int nj,
-                                                    const unsigned *__restrict__ tkey,
+                                                    int lg, const float4 *__restrict__ spred,
+                                                    int nj, const unsigned *__restrict__ tkey,
                                                     float *bound) {
-  const int lane = threadIdx.x & 31;
-  const int g = blockIdx.x * kBoundWarps + (threadIdx.x >> 5);
-  if (g >= ni) return;  // the whole warp
+  const int L = 1 << lg;
+  const int sub = threadIdx.x & (L - 1);
+  const int gt = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) >> lg);
+  const bool valid = gt < ni;  // uniform within a group
+  const int g = valid ? gt : ni - 1;  // past the end: repeat the last i, write nothing
   const int ntiles = (nj + kTJ - 1) / kTJ;
   const unsigned k = ikey[g];
   int lo = 0, hi = ntiles;  // first tile with tkey > k lies in [lo, hi]
@@ -226,12 +229,12 @@ __global__ void __launch_bounds__(256) bound_kernel(const double *__restrict__ i
   const int cnt = min(kTJ, nj - t * kTJ);
   const float4 *rec = spred + (size_t)t * kTJ * RS;
   float m = FLT_MAX;
-  for (int q = lane; q < cnt; q += 32) {
+  for (int q = sub; q < cnt; q += L) {
     float dx, dy, dz;
     m = fminf(m, pair_dr_mix(I, rec[q * RS + 0], rec[q * RS + 1], dx, dy, dz));
   }
-  for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0) bound[g] = m;
+  for (int o = L >> 1; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (valid && sub == 0) bound[g] = m;
 }
 
 }  // namespace sapb
@@ -391,13 +394,18 @@ int spatial_prepare(sapb_dev *d, int nj, int ni, const double *i_dev) {
   if (e == cudaSuccess) {
     const int is = i_stride(d->order);
     const float4 *sp4 = static_cast<const float4 *>(S.spred);
-    const int nb = (ni + kBoundWarps - 1) / kBoundWarps;
+    // lanes per i: enough threads to fill every SM (2048 each), at most 32
+    const long want = (long)d->num_sms * 2048;
+    int lg = 0;
+    while (lg < 5 && ((long)ni << lg) < want) lg++;
+    const long threads = (long)ni << lg;
+    const int nb = (int)((threads + 255) / 256);
     if (rs == 4)
-      bound_kernel<4><<<nb, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, sp4, nj, S.tkey,
-                                          S.ibound);
+      bound_kernel<4><<<nb, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, lg, sp4, nj,
+                                          S.tkey, S.ibound);
     else
-      bound_kernel<3><<<nb, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, sp4, nj, S.tkey,
-                                          S.ibound);
+      bound_kernel<3><<<nb, 256, 0, st>>>(i_dev, is, S.iidx[1], S.ikey[1], ni, lg, sp4, nj,
+                                          S.tkey, S.ibound);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess)
