@@ -362,23 +362,19 @@ __global__ void __launch_bounds__(kBT, (FCfg<ORDER, PREC, TPI, IP>::MIN_BLOCKS))
           SAPB_UNROLL(SAPB_JUNROLL)
           for (int k = ty; k < cnt; k += TPI) {
             const float4 r0 = rec[k * C::RS + 0];
-            const float4 r1 = rec[k * C::RS + 1];
             const float4 r2 = rec[k * C::RS + 2];
             const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
 #pragma unroll
-            for (int q = 0; q < NPAIR; q++)
-              pair_mix2_far<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q]);
+            for (int q = 0; q < NPAIR; q++) pair_mix2_far<ORDER>(I2[q], r0, r2, r3, eps2v, Q[q]);
           }
         } else if (far) {
           SAPB_UNROLL(SAPB_JUNROLL)
           for (int k = ty; k < cnt; k += TPI) {
             const float4 r0 = rec[k * C::RS + 0];
-            const float4 r1 = rec[k * C::RS + 1];
             const float4 r2 = rec[k * C::RS + 2];
             const float4 r3 = ORDER >= SIXTH ? rec[k * C::RS + 3] : r2;
 #pragma unroll
-            for (int q = 0; q < NPAIR; q++)
-              pair_mix2_far<ORDER>(I2[q], r0, r1, r2, r3, eps2v, Q[q]);
+            for (int q = 0; q < NPAIR; q++) pair_mix2_far<ORDER>(I2[q], r0, r2, r3, eps2v, Q[q]);
           }
         } else {
           SAPB_UNROLL(SAPB_JUNROLL)

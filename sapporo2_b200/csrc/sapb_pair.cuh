@@ -24,10 +24,12 @@ __device__ __forceinline__ void store_record(void *pred, int k, double px, doubl
     const float hx = (float)px, hy = (float)py, hz = (float)pz;
     const float lx = (float)(px - (double)hx), ly = (float)(py - (double)hy),
                 lz = (float)(pz - (double)hz);
+    // The id goes into r[1].w and again into r[2].w, so that far tiles, which
+    // need no low parts, read no r[1].
     float4 *r = reinterpret_cast<float4 *>(pred) + (size_t)k * pred_fields(ORDER);
     r[0] = make_float4(hx, hy, hz, (float)m);
     r[1] = make_float4(lx, ly, lz, __int_as_float(id));
-    r[2] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
+    r[2] = make_float4((float)vx, (float)vy, (float)vz, __int_as_float(id));
     if (ORDER >= SIXTH) r[3] = make_float4((float)ax, (float)ay, (float)az, 0.f);
   }
 }
@@ -294,17 +296,17 @@ __device__ __forceinline__ void pair_mix2(const IMix2 &I, const float4 &r0, cons
 // is not needed: the caller checks that against the i's bounds).  No
 // distance minimum is kept either: the caller rescans a far tile for list
 // members when the tile's box comes within h2 of the i.  The self pair is
-// still masked by id.
+// still masked by id, read from the record's velocity row (r2.w), so a far
+// pair reads three of the record's four float4 (6th order; two of three at 4th).
 template <int ORDER>
-__device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, const float4 &r1,
-                                              const float4 &r2, const float4 &r3, float2 eps2,
-                                              AccMix2 &A) {
+__device__ __forceinline__ void pair_mix2_far(const IMix2 &I, const float4 &r0, const float4 &r2,
+                                              const float4 &r3, float2 eps2, AccMix2 &A) {
   Pre2 P;
   P.dx = __fadd2_rn(bc2(r0.x), I.nxh);
   P.dy = __fadd2_rn(bc2(r0.y), I.nyh);
   P.dz = __fadd2_rn(bc2(r0.z), I.nzh);
   if (ORDER != GRAPE5) {
-    const int idj = __float_as_int(r1.w);
+    const int idj = __float_as_int(r2.w);  // the id's copy beside the velocity
     P.dx.x = (idj == I.ida) ? 1.0e18f : P.dx.x;
     P.dx.y = (idj == I.idb) ? 1.0e18f : P.dx.y;
   }
