@@ -103,6 +103,33 @@ def test_spatial_foreign_i_outside_the_j_box(gpu):
         assert abs(d[0] - d[1]) <= 1e-6 * d[1], (q, d)
 
 
+def test_spatial_self_pair_on_a_far_tile(gpu):
+    """i given far from their own j (same id, positions displaced by 40):
+    the self pair then lies on a far tile, whose loop reads the id from the
+    record's velocity row, and is skipped by id as the reference skips it
+    (kernels.cu:565).  Its force would shift acc and pot by ~2.5e-4."""
+    from oracle import oracle as O
+    case = T.build_case(2, 4000, seed=29, binaries=0.1)
+    n = case["n"]
+    sel = np.arange(0, n, 4)
+    xi = case["px"][sel] + np.array([40.0, -25.0, 10.0])
+    vi, ai = case["pv"][sel], case["pa"][sel]
+    h2 = np.full(len(sel), 0.01)
+    want = O.force(2, xi, vi, ai, h2, case["id"][sel], case["px"], case["pv"], case["pa"],
+                   case["m"], case["id"], case["eps2"], lists=True)
+    with sp.Sapporo(order=2, precision=sp.DOUBLESINGLE) as s:
+        s.set_launch(1, 4, 0)
+        s.set_spatial(EVERY_CALL, 1e-5)
+        s.set_j_particles(np.arange(n), case["id"], case["t0"], case["m"], case["x"],
+                          case["v"], case["a"], case["j"], case["s"], case["c"])
+        s.set_time(case["ti"])
+        s.start(n, case["id"][sel], xi, vi, ai, case["eps2"], h2)
+        got = s.results(n, ngb=True)
+        far, tiles = s.spatial_stats()
+    assert tiles > 0 and far > 0, (far, tiles)
+    T.check_forces(got, want, 2)
+
+
 def test_spatial_reorders_after_j_change(gpu):
     """The ordering follows the predicted records: a second call after new j
     data and a new prediction time uses them, not the first call's order."""
