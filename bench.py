@@ -499,16 +499,18 @@ def run_spatial_sizes_bench(args, torch):
     """Where the spatial mode pays: one call = prediction of all j + force
     on ni i (a random subset of the j, 6th order, mixed, lists on), timed on
     the device (median of the timed calls), with the spatial mode off (0)
-    and on for every call (2); j = 131072 and 2^20 Plummer + 10 % binaries."""
+    and on for every call (2); j = 16384, 65536, 131072 and 2^20 Plummer + 10 %
+    binaries."""
     import sapporo2_b200 as sp
     from sapporo2_b200 import ic
     sizes = [512, 1024, 2048, 4096, 8192, 16384, 65536]
     rows = []
-    for nj in (131072, 1 << 20):
+    for nj in (16384, 65536, 131072, 1 << 20):
         cfg = ic.make_config("C3", n=nj, seed=3)
         rng = np.random.default_rng(1)
         z = np.zeros((nj, 3))
-        sels = {ni: np.sort(rng.choice(nj, ni, replace=False)) for ni in sizes}
+        njsizes = [ni for ni in sizes if ni <= nj]
+        sels = {ni: np.sort(rng.choice(nj, ni, replace=False)) for ni in njsizes}
         ms = {}
         for mode in (0, 2):
             s = sp.Sapporo(order=sp.SIXTH, precision=sp.DOUBLESINGLE)
@@ -519,7 +521,7 @@ def run_spatial_sizes_bench(args, torch):
                               cfg["v"], z, z, z, z)
             s.force_prediction(nj)
             lib, dev = s.lib, s.dev
-            for ni in sizes:
+            for ni in njsizes:
                 sel = sels[ni]
                 rec = sp.pack_i_records(2, cfg["x"][sel], cfg["v"][sel], np.full(ni, 1e-4),
                                         cfg["id"][sel], z[sel])
@@ -544,7 +546,7 @@ def run_spatial_sizes_bench(args, torch):
                 ms[(mode, ni)] = float(np.median(ts))
             s.set_stream(None)
             s.close()
-        for ni in sizes:
+        for ni in njsizes:
             a, b = ms[(0, ni)], ms[(2, ni)]
             rows.append({"nj": nj, "ni": ni, "log2_pairs": round(float(np.log2(ni * nj)), 1),
                          "address_ms": a, "spatial_ms": b, "speedup": a / b})
@@ -556,7 +558,7 @@ def run_spatial_sizes_bench(args, torch):
         "value": float(np.mean(big)), "unit": "x", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 body + ds positions (near tiles) + f64 sums", "data": "synthetic",
-        "config": {"workload": "call sizes: i random subsets of j = 131072 and 2^20 (Plummer + "
+        "config": {"workload": "call sizes: i random subsets of j = 16384, 65536, 131072 and 2^20 (Plummer + "
                                "10 % binaries)", "rows": rows},
     }), flush=True)
 
@@ -727,9 +729,10 @@ def spatial_mode() -> int:
 
 def spatial_on(ni: int, nj: int) -> bool:
     """Whether a mixed-precision force call of ni x nj pairs runs in spatial
-    mode (the library's rule: mode 2, or mode 1, >= 1024 i and >= 2^28 pairs)."""
+    mode (the library's rule: mode 2, or mode 1, >= 1024 i, >= 65536 j and >= 2^28
+    pairs)."""
     m = spatial_mode()
-    return m == 2 or (m == 1 and ni >= 1024 and nj >= 1024 and ni * nj >= 1 << 28)
+    return m == 2 or (m == 1 and ni >= 1024 and nj >= 65536 and ni * nj >= 1 << 28)
 
 
 def main():

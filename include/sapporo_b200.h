@@ -248,7 +248,7 @@ int sapb_get_plan(sapb_dev *d, int ni, int nj, int *tpi, int *ip, int *nslices);
  * rescan, so neighbours and lists are unchanged; the force sums change only
  * at the rounding level (the summation order too) and do not depend on h2.
  * mode 0: off (address order, the reference's arithmetic for every pair),
- * 1: on for calls of >= 2^28 pairs and >= 1024 i (the default), 2: on for
+ * 1: on for calls of >= 2^28 pairs, >= 1024 i and >= 65536 j (the default), 2: on for
  * every call.
  * delta 0 keeps the default 1e-6; at most 1e-4.  The environment variable
  * SAPPORO_B200_SPATIAL (0, 1, 2) sets the mode at open.  A call for whose

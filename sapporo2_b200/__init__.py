@@ -415,7 +415,7 @@ class Sapporo:
     def set_spatial(self, mode=1, delta=0.0):
         """Spatial mode of the mixed-precision force calls: 0 off (address
         order, double-single difference for every pair), 1 on for calls of
-        >= 2^28 pairs and >= 1024 i (default), 2 on for every call; far tiles use the
+        >= 2^28 pairs, >= 1024 i and >= 65536 j (default), 2 on for every call; far tiles use the
         single-float difference, accurate to `delta` (0: 1e-6)."""
         for d in self.devs:
             _check(self.lib.sapb_set_spatial(d, int(mode), float(delta)), "set_spatial", d)

@@ -522,18 +522,20 @@ double *sapb_i_stage(sapb_dev *d, int ni) {
 }
 
 // Spatial mode pays for its per-call work (the i sort and bounds, the j
-// gather after each prediction) from about 2^28 pairs and 1024 i on (B200,
-// predict + force per call, neighbour lists on, i a random subset of the j:
-// 1.04-1.05 x at 2^28 to 2^30, 1.07-1.12 x from 2^31; 0.91 and 1.00 x at 2^26
-// and 2^27; block-step active sets, which are spatially clustered, gain
-// more); smaller calls run in address order.
+// gather after each prediction) from about 2^28 pairs, 1024 i and 65536 j on
+// (B200, predict + force per call, neighbour lists on, i a random subset of
+// the j: 1.04-1.06 x at 2^28 with 65536 to 262144 j, 1.07-1.12 x from 2^31;
+// 0.89-0.95 x at 2^28 with 16384 or 32768 j, 0.91-1.00 x at 2^26 and 2^27;
+// block-step active sets, which are spatially clustered, gain more);
+// smaller calls run in address order.
 constexpr double kSpatialMinPairs = 268435456.0;  // 2^28
 constexpr int kSpatialMinI = 1024;
+constexpr int kSpatialMinJ = 65536;
 
 static bool use_spatial(const sapb_dev *d, int ni, int nj) {
   if (d->prec != DOUBLESINGLE || d->sp.mode == 0) return false;
   if (d->sp.mode == 2) return true;
-  return ni >= kSpatialMinI && nj >= 4 * force_tile_j() && (double)ni * nj >= kSpatialMinPairs;
+  return ni >= kSpatialMinI && nj >= kSpatialMinJ && (double)ni * nj >= kSpatialMinPairs;
 }
 
 // Near-pair radius^2 of a mixed-precision call (FP32, compared with the

@@ -188,7 +188,7 @@ def test_spatial_grape5_order(gpu):
 
 
 def test_spatial_default_mode_threshold(gpu):
-    """Mode 1 (the default) orders only calls of >= 2^28 pairs: a small call
+    """Mode 1 (the default) orders only calls of >= 2^28 pairs and >= 65536 j: a small call
     gives bit-identical results to mode 0."""
     case = T.build_case(2, 2000, seed=26, binaries=0.1)
     got = T.run_library(case, sp.DOUBLESINGLE, spatial=(1, 0.0))
