@@ -558,8 +558,8 @@ def run_spatial_sizes_bench(args, torch):
         "value": float(np.mean(big)), "unit": "x", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 body + ds positions (near tiles) + f64 sums", "data": "synthetic",
-        "config": {"workload": "call sizes: i random subsets of j = 16384, 65536, 131072 and 2^20 (Plummer + "
-                               "10 % binaries)", "rows": rows},
+        "config": {"workload": "call sizes: i random subsets of j = 16384, 65536, 131072 and "
+                               "2^20 (Plummer + 10 % binaries)", "rows": rows},
     }), flush=True)
 
 
