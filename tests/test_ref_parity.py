@@ -193,3 +193,33 @@ def test_spatial_call_matches_reference(gpu):
     exempt = T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], ref, sel=sel)
     assert ties <= 2
     print(f"spatial call: far {far}/{tiles} {stats} nn-ties {ties} boundary {exempt}")
+
+
+def test_c3_headline_config_matches_reference(gpu):
+    """C3, the workload of the headline figure (N = 2^20 Plummer, Salpeter
+    masses, 10 % binaries 1e-6..1e-4 apart, 6th order): 2048 seeded i against
+    all 2^20 j (2^31 pairs, spatial mode by the default rule), lists and
+    nearest neighbours on, against the reference's sixth_DS; snap against the
+    oracle."""
+    _ref_ready()
+    from sapporo2_b200 import ic
+    from sapporo2_b200.direct import fp64_direct
+    cfg = ic.make_config("C3")
+    x, v, m, ids, eps2 = cfg["x"], cfg["v"], cfg["m"], cfg["id"], cfg["eps2"]
+    a, j, _ = fp64_direct(1, x, v, None, m, ids, eps2)
+    _, _, sn = fp64_direct(2, x, v, a, m, ids, eps2)
+    c = ic.crackle_from(x, a, j)
+    rpx, rpv, rpa = O.ref_predict(2, cfg["ti"], cfg["t0"], x, m, v, a, j, sn, c)
+    case = dict(order=2, n=cfg["n"], x=x, v=v, m=m, a=a, j=j, s=sn, c=c, id=ids, t0=cfg["t0"],
+                ti=cfg["ti"], px=rpx, pv=rpv, pa=rpa, h2=cfg["h2"], eps2=eps2)
+    sel = np.sort(np.random.default_rng(73).choice(case["n"], 2048, replace=False))
+    ref = _c2_ref(case, sel, sp.DOUBLESINGLE)
+    got = T.run_library(case, sp.DOUBLESINGLE, sel=sel, spatial=(1, 0.0))
+    far, tiles = got["far_tiles"]
+    assert far > 0.5 * tiles > 0  # the default rule ordered the call
+    stats = T.check_forces(got, ref, 2, fields=REF_FIELDS)
+    _snap_vs_oracle(case, got, sel=sel)
+    ties = T.check_nn(case, got["nnb"], ref, sel=sel)
+    exempt = T.check_neighbours(case, got["ngb_sets"], got["ngb_count"], ref, sel=sel)
+    assert ties <= 2 and np.median(ref["ngb_count"]) > 10
+    print(f"C3: far {far}/{tiles} {stats} nn-ties {ties} boundary {exempt}")
