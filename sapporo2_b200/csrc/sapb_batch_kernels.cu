@@ -42,6 +42,19 @@ __global__ void __launch_bounds__(256) batch_predict_kernel(BatchArgs B) {
                             v[0], v[1], v[2], a[0], a[1], a[2]);
 }
 
+// Shared-memory plan of the batch kernel: that of a 2-threads-per-i force
+// block, with a two-stage tile ring in mixed precision up to 4th order, where
+// three 256-record stages plus the FP64 running totals (57.6 KB) would hold
+// the kernel to 3 resident blocks per SM instead of the 4 its registers allow.
+template <int ORDER, int PREC>
+struct BCfg : FCfg<ORDER, PREC, 2, 2> {
+  using F = FCfg<ORDER, PREC, 2, 2>;
+  static constexpr int NS = (PREC != DOUBLE && ORDER <= FOURTH) ? 2 : kNS;
+  static constexpr int BODY =
+      NS * F::TILE_BYTES > F::RED_BYTES ? NS * F::TILE_BYTES : F::RED_BYTES;
+  static constexpr int SMEM = kHdr + BODY + F::TOT_BYTES;
+};
+
 // Persistent force kernel: each block repeatedly takes the next work item
 // (cluster, i-tile, j-slice) from the queue and evaluates it like one block
 // of force_kernel (2 i per thread, threads-per-i chosen per item).  The TMA
@@ -50,10 +63,10 @@ __global__ void __launch_bounds__(256) batch_predict_kernel(BatchArgs B) {
 template <int ORDER, int PREC>
 __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3 : 4)))
     batch_force_kernel(BatchArgs B) {
-  using C = FCfg<ORDER, PREC, 2, 2>;  // shared-memory plan with a row reduction area
+  using C = BCfg<ORDER, PREC>;  // shared-memory plan with a row reduction area
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  uint64_t *empty = full + kNS;
+  uint64_t *empty = full + C::NS;
   unsigned char *tiles = smem + kHdr;
   double *tot = reinterpret_cast<double *>(tiles + C::BODY);
   __shared__ int s_item;
@@ -65,7 +78,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3
 
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < kNS; s++) {
+    for (int s = 0; s < C::NS; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kBT / 32);
     }
@@ -137,7 +150,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3
 
     auto issue = [&](int t) {
       const int T = tbase + t;
-      const int st = T % kNS;
+      const int st = T % C::NS;
       const int cnt = min(kTJ, W.j_count - t * kTJ);
       const uint32_t bytes = (uint32_t)(cnt * C::REC);
       n_issued = T + 1;
@@ -147,9 +160,10 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3
                &full[st]);
     };
     if (tid == 0 && !broken) {
-      for (int t = 0; t < kNS && t < nt; t++) {
+      for (int t = 0; t < C::NS && t < nt; t++) {
         const int T = tbase + t;
-        if (T >= kNS && !mbar_wait_bounded(&empty[T % kNS], (uint32_t)((T / kNS - 1) & 1))) {
+        if (T >= C::NS &&
+            !mbar_wait_bounded(&empty[T % C::NS], (uint32_t)((T / C::NS - 1) & 1))) {
           broken = true;
           atomicOr(B.status, kErrWaitTimeout);
           break;
@@ -160,9 +174,9 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3
 
     for (int it = 0; it < nt; it++) {
       const int T = tbase + it;
-      const int s = T % kNS;
+      const int s = T % C::NS;
       if (!broken) {
-        if (mbar_wait_bounded(&full[s], (uint32_t)((T / kNS) & 1))) {
+        if (mbar_wait_bounded(&full[s], (uint32_t)((T / C::NS) & 1))) {
           n_landed = T + 1;
         } else {
           broken = true;
@@ -237,9 +251,9 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-      if (tid == 0 && !broken && it + kNS < nt) {
-        if (mbar_wait_bounded(&empty[s], (uint32_t)((T / kNS) & 1))) {
-          issue(it + kNS);
+      if (tid == 0 && !broken && it + C::NS < nt) {
+        if (mbar_wait_bounded(&empty[s], (uint32_t)((T / C::NS) & 1))) {
+          issue(it + C::NS);
         } else {
           broken = true;
           atomicOr(B.status, kErrWaitTimeout);
@@ -331,7 +345,7 @@ __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3
   }
   if (broken && tid == 0) {
     for (int T = n_landed; T < n_issued; T++)
-      mbar_wait_bounded(&full[T % kNS], (uint32_t)((T / kNS) & 1));
+      mbar_wait_bounded(&full[T % C::NS], (uint32_t)((T / C::NS) & 1));
   }
 }
 
@@ -366,7 +380,7 @@ __global__ void __launch_bounds__(256) batch_reduce_kernel(BatchArgs B) {
 template <int ORDER, int PREC>
 static cudaError_t launch_batch_t(const BatchArgs &B, int j_grid, int force_blocks, int i_grid,
                                   cudaStream_t st) {
-  using C = FCfg<ORDER, PREC, 2, 2>;
+  using C = BCfg<ORDER, PREC>;
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(batch_force_kernel<ORDER, PREC>,
@@ -397,7 +411,7 @@ cudaError_t launch_batch(int order, int prec, const BatchArgs &B, int j_grid, in
 
 template <int ORDER, int PREC>
 static int batch_occ_t() {
-  using C = FCfg<ORDER, PREC, 2, 2>;
+  using C = BCfg<ORDER, PREC>;
   if (cudaFuncSetAttribute(batch_force_kernel<ORDER, PREC>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) != cudaSuccess)
     return 1;
