@@ -42,19 +42,6 @@ __global__ void __launch_bounds__(256) batch_predict_kernel(BatchArgs B) {
                             v[0], v[1], v[2], a[0], a[1], a[2]);
 }
 
-// Shared-memory plan of the batch kernel: that of a 2-threads-per-i force
-// block, with a two-stage tile ring in mixed precision up to 4th order, where
-// three 256-record stages plus the FP64 running totals (57.6 KB) would hold
-// the kernel to 3 resident blocks per SM instead of the 4 its registers allow.
-template <int ORDER, int PREC>
-struct BCfg : FCfg<ORDER, PREC, 2, 2> {
-  using F = FCfg<ORDER, PREC, 2, 2>;
-  static constexpr int NS = (PREC != DOUBLE && ORDER <= FOURTH) ? 2 : kNS;
-  static constexpr int BODY =
-      NS * F::TILE_BYTES > F::RED_BYTES ? NS * F::TILE_BYTES : F::RED_BYTES;
-  static constexpr int SMEM = kHdr + BODY + F::TOT_BYTES;
-};
-
 // Persistent force kernel: each block repeatedly takes the next work item
 // (cluster, i-tile, j-slice) from the queue and evaluates it like one block
 // of force_kernel (2 i per thread, threads-per-i chosen per item).  The TMA
@@ -63,7 +50,7 @@ struct BCfg : FCfg<ORDER, PREC, 2, 2> {
 template <int ORDER, int PREC>
 __global__ void __launch_bounds__(kBT, (PREC == DOUBLE ? 1 : (ORDER >= SIXTH ? 3 : 4)))
     batch_force_kernel(BatchArgs B) {
-  using C = BCfg<ORDER, PREC>;  // shared-memory plan with a row reduction area
+  using C = FCfg<ORDER, PREC, 2, 2>;  // shared-memory plan with a row reduction area
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
   uint64_t *empty = full + C::NS;
@@ -380,7 +367,7 @@ __global__ void __launch_bounds__(256) batch_reduce_kernel(BatchArgs B) {
 template <int ORDER, int PREC>
 static cudaError_t launch_batch_t(const BatchArgs &B, int j_grid, int force_blocks, int i_grid,
                                   cudaStream_t st) {
-  using C = BCfg<ORDER, PREC>;
+  using C = FCfg<ORDER, PREC, 2, 2>;
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(batch_force_kernel<ORDER, PREC>,
@@ -411,7 +398,7 @@ cudaError_t launch_batch(int order, int prec, const BatchArgs &B, int j_grid, in
 
 template <int ORDER, int PREC>
 static int batch_occ_t() {
-  using C = BCfg<ORDER, PREC>;
+  using C = FCfg<ORDER, PREC, 2, 2>;
   if (cudaFuncSetAttribute(batch_force_kernel<ORDER, PREC>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) != cudaSuccess)
     return 1;

@@ -77,7 +77,10 @@ struct FCfg {
   static constexpr int REC = RS * FB;
   static constexpr int TILE_BYTES = kTJ * REC;
   static constexpr int RED_BYTES = TPI > 1 ? kBT * IP * kResStride * 8 : 0;
-  static constexpr int NS = kNS;  // stages of the tile ring
+  // stages of the tile ring: two for 2 i per thread in mixed precision up to
+  // 4th order, where three would hold the shape to 3 resident blocks per SM
+  // by shared memory (57.6 KB) against the 4 its registers allow
+  static constexpr int NS = (PREC != DOUBLE && ORDER <= FOURTH && IP == 2) ? 2 : kNS;
   static constexpr int BODY = NS * TILE_BYTES > RED_BYTES ? NS * TILE_BYTES : RED_BYTES;
   // mixed precision keeps its FP64 running totals in shared memory (10 per
   // i, [field][thread] so a warp's accesses are consecutive), which frees
