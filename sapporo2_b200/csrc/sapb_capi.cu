@@ -235,9 +235,32 @@ static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   const double sm_rate = d->prec == DOUBLE ? (d->order >= SIXTH ? 1.5e9 : 2.3e9)
                                            : (d->order >= SIXTH ? 3.6e9 : 5.6e9);
   const int max_ns = std::max(1, ntiles / 4);  // keep >= 4 tiles per slice
+  // Mixed precision below 2^32 pairs and 2^19 j: the shape family comes from
+  // the call size, the model above then picks the shape within it and the
+  // j-split.  B200 sweeps of every shape and j-split (4th and 6th order, 256
+  // to 65536 i on 16384 to 2^20 j) put the best shape at two i per thread
+  // with about 65536 / ni threads per i (2 to 8) from 1024 i on (4th order,
+  // 16384 x 16384: 0.45 ms against 0.66 ms for the model's free choice;
+  // 6th order, 4096 i on 16384 j: 0.21 against 0.28 ms), and at 8 threads
+  // per i or one i per thread below.  From 2^32 pairs, or with 2^19 j and
+  // more, where the j-split alone fills the GPU, the model chooses freely:
+  // (1,4) and (2,4) are then within 1 % of the best (2^20 j x 2048 i: (2,4)
+  // 4 % ahead of (8,2)).
+  bool allow[8] = {true, true, true, true, true, true, true, true};
+  if (d->prec != DOUBLE && !d->tpi && (double)ni * nj < 4294967296.0 && nj < (1 << 19)) {
+    for (bool &a : allow) a = false;
+    if (ni < 1024) {
+      allow[5] = allow[6] = allow[7] = true;  // (8,2), (16,1), (32,1)
+    } else {
+      int t = 2;
+      while (t < 8 && (long)t * 2 * ni <= 65536) t *= 2;
+      allow[t == 2 ? 3 : (t == 4 ? 4 : 5)] = true;  // (2,2), (4,2) or (8,2)
+    }
+  }
   Plan best{1, 2, 1, 1, ntiles};
   double best_t = 1e300;
   for (int q = 0; q < nshape; q++) {
+    if (d->prec != DOUBLE && !d->tpi && !allow[q]) continue;
     const int *sh = d->prec == DOUBLE ? shapes_dp[q] : shapes_mix[q];
     const int tpi = d->tpi ? d->tpi : sh[0];
     const int ip = d->ip ? d->ip : sh[1];
