@@ -257,10 +257,27 @@ static Plan make_plan(const sapb_dev *d, int ni, int nj) {
       allow[t == 2 ? 3 : (t == 4 ? 4 : 5)] = true;  // (2,2), (4,2) or (8,2)
     }
   }
+  // FP64 kernels, same call sizes (sweep of 4th and 6th order, 256 to 16384
+  // i on 16384 and 131072 j): one i per thread with 16 or 32 threads per i
+  // below 4096 i (16 from 1024 i on), (8,2) or (16,1) up to 16384 i, (8,2)
+  // above; the model's free choice was up to 1.16x off (4th order, 4096 i on
+  // 16384 j).
+  if (d->prec == DOUBLE && !d->tpi && (double)ni * nj < 4294967296.0 && nj < (1 << 19)) {
+    for (bool &a : allow) a = false;
+    if (ni < 1024) {
+      allow[4] = allow[5] = true;  // (16,1), (32,1)
+    } else if (ni < 4096) {
+      allow[4] = true;  // (16,1)
+    } else if (ni < 16384) {
+      allow[2] = allow[4] = true;  // (8,2), (16,1)
+    } else {
+      allow[2] = true;  // (8,2)
+    }
+  }
   Plan best{1, 2, 1, 1, ntiles};
   double best_t = 1e300;
   for (int q = 0; q < nshape; q++) {
-    if (d->prec != DOUBLE && !d->tpi && !allow[q]) continue;
+    if (!d->tpi && !allow[q]) continue;
     const int *sh = d->prec == DOUBLE ? shapes_dp[q] : shapes_mix[q];
     const int tpi = d->tpi ? d->tpi : sh[0];
     const int ip = d->ip ? d->ip : sh[1];
