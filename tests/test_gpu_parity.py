@@ -128,3 +128,20 @@ def test_near_pair_factor_is_checked(gpu):
                 s.set_near(bad)
         s.set_near(0.0)
         s.set_near(64.0)
+
+
+@pytest.mark.parametrize("order,precision,ni,nj,shapes", [
+    (1, sp.DOUBLESINGLE, 16384, 16384, {(4, 2)}),
+    (2, sp.DOUBLESINGLE, 4096, 16384, {(8, 2)}),
+    (2, sp.DOUBLESINGLE, 256, 131072, {(8, 2), (16, 1), (32, 1)}),
+    (2, sp.DOUBLESINGLE, 1 << 20, 1 << 20, {(1, 4), (2, 4)}),
+    (1, sp.DOUBLE, 2048, 16384, {(16, 1)}),
+    (2, sp.DOUBLE, 16384, 131072, {(8, 2)}),
+])
+def test_planner_shape_families(gpu, order, precision, ni, nj, shapes):
+    """The launch planner's shape families by call size (mid-size calls take
+    the measured best family; calls of 2^32 pairs and more the cost model's
+    free choice); any plan computes the same forces (other tests)."""
+    with sp.Sapporo(order=order, precision=precision) as s:
+        tpi, ip, ns = s.plan(ni, nj)
+    assert (tpi, ip) in shapes and ns >= 1, (tpi, ip, ns)
