@@ -216,6 +216,10 @@ static int blocks_per_sm(int order, int prec, int tpi, int ip) {
 // SM; S > 1 adds the slice reduction (S x ni records read).  The block
 // count B = i-tiles x S is chosen near a whole number of waves: a last wave
 // that holds a few blocks costs as much as a full one.
+extern "C" {
+static bool use_spatial(const sapb_dev *d, int ni, int nj);  // defined with the C ABI below
+}
+
 static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   const int tj = force_tile_j();
   const int ntiles = std::max(1, (nj + tj - 1) / tj);
@@ -245,9 +249,15 @@ static Plan make_plan(const sapb_dev *d, int ni, int nj) {
   // per i or one i per thread below.  From 2^32 pairs, or with 2^19 j and
   // more, where the j-split alone fills the GPU, the model chooses freely:
   // (1,4) and (2,4) are then within 1 % of the best (2^20 j x 2048 i: (2,4)
-  // 4 % ahead of (8,2)).
+  // 4 % ahead of (8,2)).  Calls in spatial mode keep the free choice too:
+  // there these shapes gained only 0-7 %, and the 6th-order block steps of a
+  // 262144-body system with tight binaries (200 steps, 10 % binaries
+  // 1e-6..1e-4 apart) reached t = 5.7e-4 with them against 3.13e-3 with the
+  // free choice and 3.25e-3 with FP64 forces (address order: 3.25e-3 with
+  // either planner); the cause is not known.
   bool allow[8] = {true, true, true, true, true, true, true, true};
-  if (d->prec != DOUBLE && !d->tpi && (double)ni * nj < 4294967296.0 && nj < (1 << 19)) {
+  if (d->prec != DOUBLE && !d->tpi && (double)ni * nj < 4294967296.0 && nj < (1 << 19) &&
+      !use_spatial(d, ni, nj)) {
     for (bool &a : allow) a = false;
     if (ni < 1024) {
       allow[5] = allow[6] = allow[7] = true;  // (8,2), (16,1), (32,1)
