@@ -237,13 +237,14 @@ int sapporo::set_j_particle(int address, int id, double tj, double dtj, double m
   return 0;
 }
 
-// fn(begin, end) over [0, n): chunks of at least 32768 on up to 16 threads
-// (a bulk j upload of 2^20 records packs 185 MB); a thread that cannot be
-// started runs its chunk inline.
+// fn(begin, end) over [0, n): chunks of at least kFillChunk on up to 16
+// threads (a bulk j upload of 2^20 records packs 185 MB); a thread that cannot
+// be started runs its chunk inline.
+static const int kFillChunk = 32768;
 template <class F>
 static void parallel_chunks(int n, F fn) {
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const int nt = std::max(1, std::min((int)std::min(hw, 16u), n / 32768));
+  const int nt = std::max(1, std::min((int)std::min(hw, 16u), n / kFillChunk));
   if (nt <= 1) {
     fn(0, n);
     return;
@@ -292,9 +293,15 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
   }
   predJOnHost = false;
   nj_updated = true;
-  // slots, then one staging reservation per device and a tight fill
+  // slots, then one staging reservation per device and a tight fill.  An
+  // address named twice in one call keeps its later entry, as with
+  // set_j_particle one by one; the fill of such a call runs on one thread
+  // (on several, two threads would write the same record)
   const int G = ndev();
   std::vector<int> slots((size_t)n);
+  std::vector<unsigned char> seen;
+  if (n >= 2 * kFillChunk) seen.assign((size_t)nj_max, 0);  // smaller fills run on one thread
+  bool repeats = false;
   for (int k = 0; k < n; k++) {
     const int addr = address[k];
     const int g = G == 1 ? 0 : addr % G;
@@ -305,6 +312,10 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
       staged_addr_[g].push_back(addr);
     }
     slots[k] = slot;
+    if (!seen.empty()) {
+      repeats |= seen[addr] != 0;
+      seen[addr] = 1;
+    }
   }
   std::vector<double *> bases((size_t)G, nullptr);
   for (int g = 0; g < G; g++) {
@@ -319,7 +330,7 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
   const bool six = integrationOrder > FOURTH;
   const int *sl = slots.data();
   double *const *bs = bases.data();
-  parallel_chunks(n, [=](int k0, int k1) {
+  auto fill = [=](int k0, int k1) {
     for (int k = k0; k < k1; k++) {
       const int addr = address[k];
       double *r = (G == 1 ? bs[0] : bs[addr % G]) + (size_t)sl[k] * ss;
@@ -339,7 +350,11 @@ int sapporo::set_j_particles(int n, const int *address, const int *id, const dou
           r[19 + d] = crk ? crk[3 * k + d] : 0.0;
         }
     }
-  });
+  };
+  if (repeats)
+    fill(0, n);
+  else
+    parallel_chunks(n, fill);
   return 0;
 }
 

@@ -22,6 +22,7 @@ import numpy as np
 import pytest
 
 import sapporo2_b200 as sp
+from sapporo2_b200 import ic
 from oracle import oracle as O
 from tests import cases as T
 
@@ -302,5 +303,40 @@ def test_device_lists_and_readback(fake):
             np.testing.assert_array_equal(p["acc"], case["pa"][k])
             np.testing.assert_array_equal(st["pos"], case["x"][k])
             np.testing.assert_array_equal(st["jrk"], case["j"][k])
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("devices", [[0], [0, 1]])
+def test_bulk_upload_repeated_address_keeps_call_order(fake, devices):
+    # one set_j_particles call that names an address twice keeps the later
+    # entry, as set_j_particle one by one would.  70001 entries are packed in
+    # chunks of 35001 when two threads are free; the repeated address is the
+    # last entry of the first chunk and the first of the second, where a
+    # threaded fill would write one record from two threads
+    n = 70000
+    x, v, m = ic.plummer(n, 12)
+    ids = (np.arange(n) + 100).astype(np.int32)
+    k2 = 35001
+    addr = np.concatenate([np.arange(k2), [k2 - 1], np.arange(k2, n)]).astype(np.int32)
+    rows = np.concatenate([np.arange(k2), [n], np.arange(k2, n)])
+    xr = np.vstack([x, x[k2 - 1] + [0.25, -0.5, 0.125]])[rows]
+    vr = np.vstack([v, -v[k2 - 1]])[rows]
+    mr = np.append(m, 3.0 * m[k2 - 1])[rows]
+    zero = np.zeros_like(xr)
+    s = open_class(fake, 1, devices)
+    try:
+        s.set_j_particles(addr, np.append(ids, ids[k2 - 1])[rows], np.ones(n + 1), mr, xr, vr,
+                          zero, zero)
+        s.set_time(1.0)
+        s.force_prediction(n)
+        for k in (0, k2 - 2, k2 - 1, k2, n - 1):
+            st = s.retrieve_state(k)
+            src = n if k == k2 - 1 else k
+            want_x = x[k2 - 1] + [0.25, -0.5, 0.125] if src == n else x[k]
+            want_m = 3.0 * m[k2 - 1] if src == n else m[k]
+            assert st["mass"] == want_m, k
+            np.testing.assert_array_equal(st["pos"], want_x)
+            np.testing.assert_array_equal(st["vel"], -v[k2 - 1] if src == n else v[k])
     finally:
         s.close()
