@@ -129,7 +129,8 @@ class sapporo {
   // handles, the status of the last call that can fail (0 = ok), and n calls
   // of set_j_particle in one (arrays of n, vectors [n][3]; a, jrk, snp, crk,
   // eps, t may be null for zeros): the same address rules, one staging
-  // reservation per device for all.
+  // reservation per device for all; an address given twice keeps its later
+  // entry, as with n calls of set_j_particle.
   sapb_dev *device_handle() { return dev_; }
   sapb_dev *device_handle(int k) { return k >= 0 && k < ndev() ? devs_[k] : nullptr; }
   int n_devices() const { return ndev(); }
