@@ -87,7 +87,11 @@ double *sapb_j_stage(sapb_dev *d, int n);
 int sapb_j_stage_stride(const sapb_dev *d);
 
 /* Copies the first n staged records to the device and scatters them to their
- * addresses (asynchronous).  Replaces send_j_particles_to_device + copyJInDev
+ * addresses (asynchronous).  The n records name distinct addresses: of two
+ * records for one address either may land.  The sapporo class keeps one
+ * record per address, the later values overwriting the earlier, as the
+ * reference's address map does (lib/src/sapporohostclass.cpp:476-494).
+ * Replaces send_j_particles_to_device + copyJInDev
  * (lib/src/sapporohostclass.cpp:889-923, 1204-1248). */
 int sapb_push_j(sapb_dev *d, int n);
 
