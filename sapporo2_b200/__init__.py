@@ -243,6 +243,14 @@ def _i32(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
 
 
+def _per_particle(a, n, what):
+    """`a` (already converted) as n scalars, one per particle: the C side
+    reads n values, so a shorter or longer array is refused here."""
+    if a is not None and a.shape != (n,):
+        raise ValueError(f"{what}: {n} values expected, got shape {a.shape}")
+    return a
+
+
 class Sapporo:
     """The ``sapporo`` class (C++).  Method names follow the reference; array
     arguments are numpy arrays ([n, 3] for vectors).  ``devices`` (a list of
@@ -311,21 +319,25 @@ class Sapporo:
         _check(self.lib.sapporo_c_set_no_time(self.h), "set_no_time")
 
     def set_j_particles(self, address, id, t, mass, x, v, a, jrk, snp=None, crk=None, eps=None):
-        address = _i32(address)
+        address = _i32(address).reshape(-1)
         n = len(address)
+        if mass is None or x is None:
+            raise ValueError("set_j_particles: mass and x are required")
         _check(self.lib.sapporo_c_set_j_particles(
-            self.h, n, address, _i32(id), _f64(t), _f64(mass), _f64(x, (n, 3)), _f64(v, (n, 3)),
+            self.h, n, address, _per_particle(_i32(id), n, "id"), _per_particle(_f64(t), n, "t"),
+            _per_particle(_f64(mass), n, "mass"), _f64(x, (n, 3)), _f64(v, (n, 3)),
             _f64(a, (n, 3)), _f64(jrk, (n, 3)), _f64(snp, (n, 3)) if snp is not None else None,
-            _f64(crk, (n, 3)) if crk is not None else None, _f64(eps)), "set_j_particle",
-            self.dev)
+            _f64(crk, (n, 3)) if crk is not None else None, _per_particle(_f64(eps), n, "eps")),
+            "set_j_particle", self.dev)
 
     def start(self, nj, id, xi, vi, ai=None, eps2=0.0, h2=None):
-        id = _i32(id)
+        id = _i32(id).reshape(-1)
         ni = len(id)
         _check(self.lib.sapporo_c_start(self.h, int(nj), ni, id, _f64(xi, (ni, 3)),
                                         _f64(vi, (ni, 3)),
                                         _f64(ai, (ni, 3)) if ai is not None else None,
-                                        float(eps2), _f64(h2)), "startGravCalc", self.dev)
+                                        float(eps2), _per_particle(_f64(h2), ni, "h2")),
+               "startGravCalc", self.dev)
         self._ni = ni
 
     def results(self, nj, ni=None, ngb=True) -> dict:
@@ -465,19 +477,20 @@ class G5:
         self.lib.g5_set_eps_to_all(float(eps))
 
     def set_j(self, x, m):
-        x, m = _f64(x), _f64(m)
+        m = _f64(m).reshape(-1)
+        x = _f64(x, (len(m), 3))
         self.lib.g5_set_n(len(m))
         self.lib.g5_set_xmj(0, len(m), x, m)
 
     def force(self, xi):
-        xi = _f64(xi)
+        xi = _f64(xi).reshape(-1, 3)
         a, phi = np.zeros((len(xi), 3)), np.zeros(len(xi))
         self.lib.g5_calculate_force_on_x(xi, a, phi, len(xi))
         return a, phi
 
     def force_chunk(self, xi):
         """g5_set_xi + g5_get_force (ni <= n_pipes)."""
-        xi = _f64(xi)
+        xi = _f64(xi).reshape(-1, 3)
         a, phi = np.zeros((len(xi), 3)), np.zeros(len(xi))
         self.lib.g5_set_xi(len(xi), xi)
         self.lib.g5_run()
@@ -519,32 +532,34 @@ class G6:
     def set_j_particle(self, address, index, tj, dtj, mass, k18, j6, a2, v, x, cluster=0):
         return self.lib.g6_set_j_particle_(self._i(cluster), self._i(address), self._i(index),
                                            self._d(tj), self._d(dtj), self._d(mass),
-                                           _f64(k18), _f64(j6), _f64(a2), _f64(v), _f64(x))
+                                           _f64(k18, (3,)), _f64(j6, (3,)), _f64(a2, (3,)),
+                                           _f64(v, (3,)), _f64(x, (3,)))
 
     def calc_firsthalf(self, nj, index, xi, vi, aold, j6old, phiold, eps2, h2, cluster=0):
-        index = _i32(index)
+        index = _i32(index).reshape(-1)
         ni = len(index)
         self.lib.g6calc_firsthalf_(self._i(cluster), self._i(nj), self._i(ni), index,
                                    _f64(xi, (ni, 3)), _f64(vi, (ni, 3)), _f64(aold, (ni, 3)),
-                                   _f64(j6old, (ni, 3)), _f64(phiold), self._d(eps2), _f64(h2))
+                                   _f64(j6old, (ni, 3)), _per_particle(_f64(phiold), ni, "phiold"),
+                                   self._d(eps2), _per_particle(_f64(h2), ni, "h2"))
 
     def calc_lasthalf(self, nj, index, xi, vi, eps2, h2, cluster=0):
-        index = _i32(index)
+        index = _i32(index).reshape(-1)
         ni = len(index)
         acc, jrk, pot = np.zeros((ni, 3)), np.zeros((ni, 3)), np.zeros(ni)
         rc = self.lib.g6calc_lasthalf_(self._i(cluster), self._i(nj), self._i(ni), index,
                                        _f64(xi, (ni, 3)), _f64(vi, (ni, 3)), self._d(eps2),
-                                       _f64(h2), acc, jrk, pot)
+                                       _per_particle(_f64(h2), ni, "h2"), acc, jrk, pot)
         return rc, acc, jrk, pot
 
     def calc_lasthalf2(self, nj, index, xi, vi, eps2, h2, cluster=0):
-        index = _i32(index)
+        index = _i32(index).reshape(-1)
         ni = len(index)
         acc, jrk, pot = np.zeros((ni, 3)), np.zeros((ni, 3)), np.zeros(ni)
         inn = np.zeros(ni, dtype=np.int32)
         rc = self.lib.g6calc_lasthalf2_(self._i(cluster), self._i(nj), self._i(ni), index,
                                         _f64(xi, (ni, 3)), _f64(vi, (ni, 3)), self._d(eps2),
-                                        _f64(h2), acc, jrk, pot, inn)
+                                        _per_particle(_f64(h2), ni, "h2"), acc, jrk, pot, inn)
         return rc, acc, jrk, pot, inn
 
     def read_neighbour_list(self, cluster=0):

@@ -340,3 +340,31 @@ def test_bulk_upload_repeated_address_keeps_call_order(fake, devices):
             np.testing.assert_array_equal(st["vel"], -v[k2 - 1] if src == n else v[k])
     finally:
         s.close()
+
+
+def test_wrapper_refuses_arrays_of_the_wrong_length(fake):
+    # per-particle arrays shorter or longer than the address list are refused
+    # in Python, before the C side could read past their end
+    case = T.build_case(1, 64, seed=13)
+    n = case["n"]
+    s = open_class(fake, 1, [0])
+    args = [np.arange(n), case["id"], case["t0"], case["m"], case["x"], case["v"], case["a"],
+            case["j"]]
+    try:
+        for k, what in ((1, "id"), (2, "t"), (3, "mass")):
+            bad = list(args)
+            bad[k] = args[k][:-1]
+            with pytest.raises(ValueError, match=what):
+                s.set_j_particles(*bad)
+        with pytest.raises(ValueError, match="eps"):
+            s.set_j_particles(*args, eps=np.zeros(n + 1))
+        with pytest.raises(ValueError):
+            s.set_j_particles(*args[:4], case["x"][:-1], *args[5:])
+        s.set_j_particles(*args)
+        s.set_time(case["ti"])
+        with pytest.raises(ValueError, match="h2"):
+            s.start(n, case["id"], case["px"], case["pv"], None, case["eps2"], case["h2"][:-1])
+        s.start(n, case["id"], case["px"], case["pv"], None, case["eps2"], case["h2"])
+        s.results(n)
+    finally:
+        s.close()
