@@ -44,6 +44,10 @@ int sapporo_c_results(sapporo_c *s, int nj, int ni, double *acc, double *jrk, do
 int sapporo_c_force_prediction(sapporo_c *s, int nj);
 int sapporo_c_read_ngb_list(sapporo_c *s);
 int sapporo_c_get_ngb_list(sapporo_c *s, int ipipe, int maxlength, int *nblen, int *nbl);
+/* How many ids the last sapporo_c_get_ngb_list wrote to nbl (sorted): *nblen
+ * capped at maxlength, less the ids beyond NGB_PB of an overflowing device's
+ * list (which were not stored). */
+int sapporo_c_ngb_list_copied(sapporo_c *s);
 /* out: mass, id, eps2, pos[3], vel[3], acc[3] (10 doubles). */
 int sapporo_c_retrieve_predicted(sapporo_c *s, int addr, double *out);
 /* out: mass, id, eps2, pos[3], vel[3], acc[3], jrk[3], ppos[3], pvel[3], pacc[3] (24). */

@@ -77,6 +77,7 @@ class sapporo {
   std::vector<std::vector<int> > ngb_count_h_;  // per device
   std::vector<std::vector<int> > ngb_list_h_;
   bool ngb_fetched_;
+  int ngb_copied_;               // ids written by the last get_ngb_list
 
   int ndev() const { return (int)devs_.size(); }
   int nj_on(int g, int nj) const;  // j among the first nj addresses held by device g
@@ -134,6 +135,9 @@ class sapporo {
   sapb_dev *device_handle() { return dev_; }
   sapb_dev *device_handle(int k) { return k >= 0 && k < ndev() ? devs_[k] : nullptr; }
   int n_devices() const { return ndev(); }
+  // the number of ids the last get_ngb_list wrote to nbl (sorted): nblen
+  // capped at maxlength, less any ids beyond NGB_PB of a device's list
+  int ngb_list_copied() const { return ngb_copied_; }
   int last_status;
   int set_j_particles(int n, const int *address, const int *id, const double *t,
                       const double *mass, const double *x, const double *v, const double *a,

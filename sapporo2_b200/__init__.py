@@ -141,6 +141,7 @@ _SIGS = [
     ("sapporo_c_force_prediction", C.c_int, [C.c_void_p, C.c_int]),
     ("sapporo_c_read_ngb_list", C.c_int, [C.c_void_p]),
     ("sapporo_c_get_ngb_list", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), _ip]),
+    ("sapporo_c_ngb_list_copied", C.c_int, [C.c_void_p]),
     ("sapporo_c_retrieve_predicted", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("sapporo_c_retrieve_state", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("sapporo_c_last_status", C.c_int, [C.c_void_p]),
@@ -402,7 +403,8 @@ class Sapporo:
         buf = np.zeros(max(maxlength, 1), dtype=np.int32)
         n = C.c_int(0)
         ovf = self.lib.sapporo_c_get_ngb_list(self.h, int(ipipe), int(maxlength), C.byref(n), buf)
-        return ovf, n.value, buf[:min(n.value, maxlength, NGB_PB)].copy()
+        # the ids written: several devices' lists together may hold more than NGB_PB
+        return ovf, n.value, buf[:self.lib.sapporo_c_ngb_list_copied(self.h)].copy()
 
     def retrieve_predicted(self, addr: int) -> dict:
         o = np.zeros(12)
@@ -570,7 +572,11 @@ class G6:
         n = C.c_int(0)
         ovf = self.lib.g6_get_neighbour_list_(self._i(cluster), self._i(ipipe),
                                               self._i(maxlength), C.byref(n), buf)
-        return ovf, n.value, buf[:min(n.value, maxlength, NGB_PB)].copy()
+        # without overflow every id counted was written (several devices'
+        # lists together may exceed NGB_PB); with it, at least the first
+        # min(count, maxlength, NGB_PB)
+        k = n.value if ovf == 0 else min(n.value, maxlength, NGB_PB)
+        return ovf, n.value, buf[:k].copy()
 
 
 class Batch:

@@ -84,6 +84,7 @@ int sapporo_c_get_ngb_list(sapporo_c *s, int ipipe, int maxlength, int *nblen, i
   if (!s || !nblen) return SAPB_EINVAL;
   return s->obj.get_ngb_list(0, ipipe, maxlength, *nblen, nbl);
 }
+int sapporo_c_ngb_list_copied(sapporo_c *s) { return s ? s->obj.ngb_list_copied() : 0; }
 
 int sapporo_c_retrieve_predicted(sapporo_c *s, int addr, double *out) {
   if (!s || !out) return SAPB_EINVAL;

@@ -66,6 +66,7 @@ sapporo::sapporo()
       dev_ni(0),
       nj_last_(0),
       ngb_fetched_(false),
+      ngb_copied_(0),
       last_status(0) {}
 
 sapporo::~sapporo() { close(); }
@@ -557,6 +558,7 @@ int sapporo::get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, 
   // lib/src/sapporohostclass.cpp:837-880: the devices' lists in device order,
   // overflow once the total reaches maxlength; then sorted
   nblen = 0;
+  ngb_copied_ = 0;
   if (!ngb_fetched_) fetch_ngb_list_from_device(cluster_id);
   if (ipipe < 0 || ipipe >= dev_ni || !ngb_fetched_) return 1;
   bool overflow = false;
@@ -574,6 +576,7 @@ int sapporo::get_ngb_list(int cluster_id, int ipipe, int maxlength, int &nblen, 
     }
   }
   std::sort(nbl, nbl + copied);
+  ngb_copied_ = copied;
   if (overflow && verbose())
     fprintf(stderr, "sapporo::get_ngb_list(..) - overflow for ipipe= %d, ngb= %d\n", ipipe, nblen);
   return overflow;

@@ -219,6 +219,13 @@ def test_list_overflow_rules(fake):
                 break
         assert nb == total and len(ids) == min(total, 10)
         assert ovf == int(total >= 10)
+    # maxlength above NGB_PB: the devices' lists together (400 ids for the
+    # first 20 i) come back whole and sorted
+    long = run(fake, case, list(range(G)), sel, maxlength=1024, h2=h2)
+    for q, (ovf, nb, ids) in enumerate(long["lists"]):
+        assert ovf == 0 and nb == per_dev[q].sum() and len(ids) == nb
+        np.testing.assert_array_equal(ids, np.sort(case["id"][inside[q]]))
+    assert max(len(ids) for _, _, ids in long["lists"]) > sp.NGB_PB
 
 
 def test_g6_interface_over_devices(fake):
