@@ -245,8 +245,9 @@ def _i32(a):
 
 
 def _per_particle(a, n, what):
-    """`a` (already converted) as n scalars, one per particle: the C side
-    reads n values, so a shorter or longer array is refused here."""
+    """`a` (already converted) as n scalars, one per particle (or per
+    cluster): the C side reads n values, so a shorter or longer array is
+    refused here."""
     if a is not None and a.shape != (n,):
         raise ValueError(f"{what}: {n} values expected, got shape {a.shape}")
     return a
@@ -611,9 +612,14 @@ class Batch:
         self.close()
 
     def plan(self, j_first, j_count, i_count, t_pred=None, eps2=None):
+        j_first = _i32(j_first).reshape(-1)
         n = len(j_first)
-        _check(self.lib.sapb_batch_plan(self.h, n, _i32(j_first), _i32(j_count), _i32(i_count),
-                                        _f64(t_pred), _f64(eps2)), "batch_plan", self.owner.dev)
+        _check(self.lib.sapb_batch_plan(self.h, n, j_first,
+                                        _per_particle(_i32(j_count), n, "j_count"),
+                                        _per_particle(_i32(i_count), n, "i_count"),
+                                        _per_particle(_f64(t_pred), n, "t_pred"),
+                                        _per_particle(_f64(eps2), n, "eps2")),
+               "batch_plan", self.owner.dev)
         self.total_i = int(np.sum(i_count))
 
     def run(self, flags=F_PREDICT):
