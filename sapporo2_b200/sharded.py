@@ -72,7 +72,9 @@ def merge_lists(counts, lists, ipipe: int, maxlength: int = NGB_PB):
     and lists [W, ni, NGB_PB]: concatenated in rank order, each rank giving
     min(its count, NGB_PB, room left) ids; overflow when the running total
     reaches maxlength (sapporo::get_ngb_list, lib/src/sapporohostclass.cpp:
-    837-880).  Returns (overflow, total count, sorted ids)."""
+    837-880) or a rank's count reaches NGB_PB (its ids beyond NGB_PB were not
+    stored), as the class does over its devices.  Returns (overflow, total
+    count, sorted ids)."""
     out = []
     nblen = 0
     overflow = False
@@ -81,6 +83,8 @@ def merge_lists(counts, lists, ipipe: int, maxlength: int = NGB_PB):
         take = max(0, min(n, NGB_PB, maxlength - nblen))
         out.append(lists[r, ipipe, :take])
         nblen += n
+        if n >= NGB_PB:
+            overflow = True
         if nblen >= maxlength:
             overflow = True
             break

@@ -92,6 +92,14 @@ def test_merge_lists_follows_the_device_order_and_overflow_rule():
     assert (ovf, n, list(ids)) == (True, 5, [1, 4, 7, 9])
     ovf, n, ids = merge_lists(counts, lists, 1, NGB_PB)  # 300 in total
     assert ovf and n == 300 and len(ids) == NGB_PB
+    # maxlength above NGB_PB: 300 ids from two ranks below NGB_PB each come
+    # back whole; a rank holding NGB_PB or more flags overflow (its ids beyond
+    # NGB_PB were not stored) although the total stays below maxlength
+    ovf, n, ids = merge_lists(counts, lists, 1, 1024)
+    assert not ovf and n == 300 and len(ids) == 300
+    big = np.array([[3, 260], [2, 10]])
+    ovf, n, ids = merge_lists(big, lists, 1, 1024)
+    assert ovf and n == 270 and len(ids) == NGB_PB + 10
 
 
 def test_two_gloo_ranks_match_one_oracle_holding_every_j():
