@@ -10,8 +10,12 @@ Python integrators can drive it:
 * :class:`G6` -- the GRAPE-6 functions (reference
   lib/interfaces/sapporoG6lib.cpp), called exactly as a C/Fortran caller
   would;
-* :class:`Device` -- the lower sapb_* C ABI (``include/sapporo_b200.h``),
-  including device-resident force calls for callers that keep data on the GPU.
+* :class:`G5` -- the GRAPE-5 functions (reference lib/interfaces/sapporoG5lib.cpp);
+* :class:`Batch` -- batched force calls over many clusters (``sapb_batch_*``);
+* the lower sapb_* C ABI (``include/sapporo_b200.h``) through ``_SIGS``
+  (``load_library()`` returns the bound library; :class:`Sapporo` exposes the
+  handles of its devices as ``dev`` / ``devs``), including the device-resident
+  force calls ``sapb_force_device`` and ``sapb_force_device_noalloc``.
 
 There is no CPU fallback: if the library is missing or no sm_100 GPU is
 present the calls raise.
