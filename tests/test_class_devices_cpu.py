@@ -375,3 +375,22 @@ def test_wrapper_refuses_arrays_of_the_wrong_length(fake):
         s.results(n)
     finally:
         s.close()
+    # the GRAPE-6 wrapper: 3-vectors of a j particle and per-i h2 / phiold
+    g6 = sp.G6.__new__(sp.G6)
+    g6.lib = fake
+    assert g6.open_special((0,)) == 0
+    try:
+        z3, zi = np.zeros(3), np.zeros((n, 3))
+        with pytest.raises(ValueError):
+            g6.set_j_particle(0, 5, 0.0, 0.0, 1.0, z3, z3, z3, z3, np.zeros(2))
+        with pytest.raises(ValueError, match="h2"):
+            g6.calc_firsthalf(n, case["id"], case["px"], case["pv"], zi, zi, np.zeros(n),
+                              case["eps2"], case["h2"][:-1])
+        with pytest.raises(ValueError, match="phiold"):
+            g6.calc_firsthalf(n, case["id"], case["px"], case["pv"], zi, zi, np.zeros(n - 1),
+                              case["eps2"], case["h2"])
+        with pytest.raises(ValueError, match="h2"):
+            g6.calc_lasthalf2(n, case["id"], case["px"], case["pv"], case["eps2"],
+                              case["h2"][:-1])
+    finally:
+        g6.close()
